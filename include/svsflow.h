@@ -1,0 +1,202 @@
+/*
+ * svsflow.h - C ABI of the B200 (sm_100a) 3D TV-L1 optical-flow and mask-propagation library
+ * (libsvsflow.so).
+ *
+ * It replaces the reference's pybind module `opticalFlow_cuda_ext.opticalFlow`
+ * (svs/src/bindings.cpp:16-192, 3D subset) and the per-pair solver loop of
+ * svs/modules/flow/tvl13d.py:122-255. All pointers are DEVICE pointers unless a comment says
+ * otherwise; sizes are element counts; every call is asynchronous on the given stream
+ * (NULL = the legacy default stream, which is where the reference launched its kernels).
+ *
+ * Layouts are the reference's: C-order, components last.
+ *   scalar field  [NZ,NY,NX]          vector field [NZ,NY,NX,3]
+ *   matrix field  [NZ,NY,NX,3,3]      (row = flow component, column = derivative x,y,z)
+ *   CNN volume    [B,C,NZ,NY,NX]      flow for CNN warp [B,NZ,NY,NX,3]
+ * Vector component 0 is x (fastest axis), 1 is y, 2 is z.
+ *
+ * Errors: every entry point returns an svs_status. On failure, svs_last_error() returns a
+ * thread-local message. The reference raised c10::Error (TORCH_CHECK / CHECK_INPUT,
+ * svs/src/coreDefines.h:10-12) and ignored launch errors (svs/src/cudaDebug.cuh:15-27); here
+ * argument errors and launch errors are both reported.
+ */
+#ifndef SVSFLOW_H_
+#define SVSFLOW_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* svs_stream_t; /* == cudaStream_t */
+
+typedef enum {
+  SVS_OK = 0,
+  SVS_ERR_INVALID_ARG = 1,
+  SVS_ERR_OUT_OF_MEMORY = 2,
+  SVS_ERR_LAUNCH = 3,
+  SVS_ERR_TIMEOUT = 4,
+  SVS_ERR_UNSUPPORTED = 5,
+  SVS_ERR_CUDA = 6
+} svs_status;
+
+/* svs/src/boundary.cuh:13-21 */
+enum { SVS_BOUNDARY_NEAREST = 0, SVS_BOUNDARY_MIRROR = 1, SVS_BOUNDARY_REFLECT = 2 };
+/* svs/src/coreDefines.h:94-100 */
+enum { SVS_INTERPOLATE_NEAREST = 0, SVS_INTERPOLATE_LINEAR = 1, SVS_INTERPOLATE_CUBIC_HERMITESPLINE = 2 };
+/* storage precision of the fused solver's state (arithmetic is always FP32) */
+enum { SVS_STORAGE_F32 = 0, SVS_STORAGE_BF16 = 1, SVS_STORAGE_F16 = 2 };
+
+const char* svs_last_error(void);
+int svs_version(void);
+
+/* ---------------------------------------------------------------------------------------------
+ * Per-operator entry points (one reference op each). h = mesh spacing L/(N-1) per axis.
+ * ------------------------------------------------------------------------------------------- */
+
+/* Nabla3D_CD.forward (svs/src/differentialOps.h:82-85; kernels differentialOps.cu:540-655)
+ * and .forwardVectorField (:90-93; differentialOps.cu:782-907): central-difference gradient of
+ * each of the C components of b [NZ,NY,NX,C] into out [NZ,NY,NX,C,3]. C = 1 is .forward. */
+svs_status svs_nabla3d_forward(const float* b, int nz, int ny, int nx, int C, float hz, float hy,
+                               float hx, int boundary, float* out, svs_stream_t stream);
+
+/* Nabla3D_CD.backward / .backwardVectorField (differentialOps.h:86-89, :94-97; kernels
+ * differentialOps.cu:658-779, :909-1039): adjoint of the gradient, p [NZ,NY,NX,C,3] -> out
+ * [NZ,NY,NX,C]. */
+svs_status svs_nabla3d_backward(const float* p, int nz, int ny, int nx, int C, float hz, float hy,
+                                float hx, int boundary, float* out, svs_stream_t stream);
+
+/* AnisotropicNabla3D.computeTangentVecs (anisotropicDifferentialOps.h:414-420; kernel
+ * anisotropicDifferentialOps.cu:89-141): g [n,3] -> s [n], normals, t1, t2 [n,3]. */
+svs_status svs_aniso3d_tangents(const float* g, int64_t n, float alpha, float beta, float* s,
+                                float* normals, float* t1, float* t2, svs_stream_t stream);
+
+/* AnisotropicNabla3D.forwardVectorField / .backwardVectorField (identical in the reference,
+ * anisotropicDifferentialOps.h:422-444; kernel anisotropicDifferentialOps.cu:143-175):
+ * out[c][d] = s (n.in_c) n[d] + (t1.in_c) t1[d] for in/out [n,3,3]. t2 is accepted and unused
+ * (its factor is never accumulated in the reference). */
+svs_status svs_aniso3d_apply(const float* in, int64_t n, const float* s, const float* normals,
+                             const float* t1, const float* t2, float* out, svs_stream_t stream);
+
+/* TVL1OF3D_proxPrimal (opticalFlowOps.h:111-120; kernel opticalFlowOps.cu:123-175). */
+svs_status svs_tvl1_prox_primal(const float* primal, int64_t n, float tau, float weight_matching,
+                                const float* rho, const float* i1w_grad, float* out,
+                                svs_stream_t stream);
+
+/* TVL1OF3D_proxDual (opticalFlowOps.h:123-129; kernel opticalFlowOps.cu:179-208). sigma is
+ * accepted and unused, as in the reference. */
+svs_status svs_tvl1_prox_dual(const float* dual, int64_t n, float sigma, float weight_tv,
+                              float* out, svs_stream_t stream);
+
+/* Warping3D.forward / .forwardVectorField (warpingOps.h:87-116; kernels warpingOps.cu:572-660
+ * and their nearest/trilinear siblings): out(x) = u(x + phi(x)) for u [NZ,NY,NX,C],
+ * phi [NZ,NY,NX,3]. */
+svs_status svs_warp3d(const float* u, int nz, int ny, int nx, int C, const float* phi, float hz,
+                      float hy, float hx, int interpolation, int boundary, float* out,
+                      svs_stream_t stream);
+
+/* Warping3D.backward (warpingOps.h:103-108; kernels warpingOps.cu:172-200, :384-412, :598-630;
+ * interpolation_*.cuh 3D backward helpers): gradients of sum(grad_out * warp(u, phi)) with
+ * respect to u [NZ,NY,NX] (scattered with atomic adds onto the folded stencil nodes, as the
+ * reference does) and phi [NZ,NY,NX,3] (the derivative of the interpolant at the sample point
+ * divided by h; zero for nearest). grad_u and grad_phi are overwritten. Scalar fields only, as
+ * in the reference. */
+svs_status svs_warp3d_backward(const float* u, int nz, int ny, int nx, const float* phi,
+                               const float* grad_out, float hz, float hy, float hx,
+                               int interpolation, int boundary, float* grad_u, float* grad_phi,
+                               svs_stream_t stream);
+
+/* WarpingCNN3D.forward (warpingOpsCNN.h:240-263; kernel warpingOpsCNN.cu:97-128):
+ * out[b,c] = m[b,c](x + phi[b](x)) for m [B,C,NZ,NY,NX], phi [B,NZ,NY,NX,3]. */
+svs_status svs_warp_cnn3d(const float* m, int B, int C, int nz, int ny, int nx, const float* phi,
+                          float hz, float hy, float hx, int interpolation, int boundary,
+                          float* out, svs_stream_t stream);
+
+/* Prolongation3D.forward / .forwardVectorField / .forwardMatrixField (prolongationOps.h:79-107;
+ * kernels prolongationOps.cu:533-625): resample a C-component field from mesh (n*, L*) to mesh
+ * (t*, tL*); target node i samples the source at (i*h_t)*L_s/L_t. */
+svs_status svs_prolongate3d(const float* u, int nz, int ny, int nx, int C, float lz, float ly,
+                            float lx, int tz, int ty, int tx, float tlz, float tly, float tlx,
+                            int interpolation, int boundary, float* out, svs_stream_t stream);
+
+/* apply_gaussian_blur3d (svs/utils/flow_utils.py:94-112): zero-padded 3D correlation of
+ * in [NZ,NY,NX] with a (2r+1)^3 kernel given in HOST memory (weights_host, float32). */
+svs_status svs_gauss_blur3d(const float* in, int nz, int ny, int nx, const float* weights_host,
+                            int r, float* out, svs_stream_t stream);
+
+/* apply_median_filter (svs/utils/flow_utils.py:115-132): ks^3 median (ks = 3 or 5) of each
+ * component of in [NZ,NY,NX,C], scipy 'reflect' boundary. Replaces the reference's host round
+ * trip through scipy. */
+svs_status svs_median3d(const float* in, int nz, int ny, int nx, int C, int ks, float* out,
+                        svs_stream_t stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Fused solver: TVL13DOpticalFlow.compute (svs/modules/flow/tvl13d.py:122-162) for a batch of
+ * independent frame pairs. Every pair is solved from zero flow at the coarsest level (the
+ * reference's warm start is overwritten when num_scales > 1, tvl13d.py:150, 158).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct svs_tvl1_params {
+  int num_scales;            /* tvl13d.py:55 */
+  int max_warps;             /* :56 */
+  int max_outer_iterations;  /* :57 */
+  float weight_matching;     /* :58 (lambda of the L1 data term) */
+  float weight_tv;           /* :59 (radius of the dual ball) */
+  int primaldual_algorithm_type; /* :60 (1: fixed steps, 2: accelerated schedule) */
+  double sigma, tau, theta, gamma; /* :61 (theta is never used for extrapolation) */
+  int use_anisotropic_diff;  /* :62 */
+  float alpha, beta;         /* :63 */
+  int use_gaussian_blur;     /* :64 */
+  float gaussian_blur_sigma; /* :65 */
+  int interpolation;         /* :68 (solver kernels require CUBIC_HERMITESPLINE) */
+  int boundary;              /* :68 */
+  int length_type;           /* 0 = numDofs (L = N-1, h = 1), 1 = fixed lengths below */
+  float length_z, length_y, length_x;
+  int median_kernel;         /* 0 = off, else the processor's post-filter size (processor.py:116) */
+  int storage;               /* SVS_STORAGE_* for the iteration state */
+} svs_tvl1_params;
+
+typedef struct svs_pair_desc {
+  int nz, ny, nx;
+  const float* I0; /* [nz,ny,nx] fixed frame (processor.py:111: img[t_{j+1}]) */
+  const float* I1; /* [nz,ny,nx] moving frame (processor.py:112: img[t_j]) */
+  float* u_out;    /* [nz,ny,nx,3] flow */
+  float* p_out;    /* [nz,ny,nx,3,3] dual field, or NULL */
+  const float* u_init; /* [nz,ny,nx,3] warm start or NULL; used only when num_scales == 1 */
+  const float* p_init; /* [nz,ny,nx,3,3] warm start or NULL; used only when num_scales == 1 */
+} svs_pair_desc;
+
+typedef struct svs_plan svs_plan;
+
+/* Create a plan for a batch of up to max_pairs pairs whose level-0 sizes are listed in
+ * dims[3*i .. 3*i+2] (nz, ny, nx). The plan owns all device state (pyramids, dual fields,
+ * linearisation) and one CUDA graph of the whole batched solve, built on first use. */
+svs_status svs_tvl1_plan_create(const svs_tvl1_params* params, int num_pairs,
+                                const int* dims_host, svs_plan** plan);
+svs_status svs_tvl1_plan_destroy(svs_plan* plan);
+/* Bytes of device memory the plan holds. */
+size_t svs_tvl1_plan_device_bytes(const svs_plan* plan);
+/* Select the iteration tile (0 = automatic) for later solves; returns SVS_ERR_INVALID_ARG for
+ * an unknown id. Used by the autotuner. */
+svs_status svs_tvl1_plan_set_tile(svs_plan* plan, int tile_id);
+int svs_tvl1_num_tiles(void);
+
+/* Solve every pair of the plan (pairs[i] must match dims[i] of the plan). */
+svs_status svs_tvl1_solve_batch(svs_plan* plan, const svs_pair_desc* pairs_host, int num_pairs,
+                                svs_stream_t stream);
+
+/* Benchmark hook: launch `count` iterate kernels (the fused primal-dual iteration) of pyramid
+ * level `level` on the plan's current state, alternating its ping-pong buffers. Used to time the
+ * dominant kernel on live data; it overwrites the plan's iteration state (results already copied
+ * out by svs_tvl1_solve_batch are unaffected). Requires one earlier solve. */
+svs_status svs_tvl1_bench_iterations(svs_plan* plan, int level, int count, svs_stream_t stream);
+/* Number of kernel nodes in the plan's captured solve graph (0 before the first solve). */
+uint64_t svs_tvl1_plan_graph_kernels(const svs_plan* plan);
+
+/* Kernel-launch counter (all kernels this library launched in this process), for benchmarks. */
+uint64_t svs_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SVSFLOW_H_ */

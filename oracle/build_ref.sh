@@ -1,0 +1,36 @@
+#!/usr/bin/env bash
+# Builds the reference CUDA extension (opticalFlow_cuda_ext.opticalFlow) for sm_100a from the
+# reference sources, so that the GPU tests can pin the oracle against the reference itself.
+# Test infrastructure only: nothing in the product links or imports the result.
+#
+# The reference sources are read in place and copied to a scratch folder under /tmp, where one
+# token is patched (`.type()` -> `.scalar_type()` inside AT_DISPATCH_FLOATING_TYPES, which the
+# reference's torch 2.1 accepted and torch 2.11 rejects). No source is copied into this repo.
+# Output: oracle/_ref/opticalFlow_cuda_ext/opticalFlow*.so (git-ignored, travels with the repo).
+set -euo pipefail
+REF_SRC=${REF_SRC:-/root/reference/svs/src}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT="$HERE/_ref/opticalFlow_cuda_ext"
+if [ ! -d "$REF_SRC" ]; then
+  echo "reference sources not found at $REF_SRC; nothing to build" >&2
+  exit 0
+fi
+SCRATCH=$(mktemp -d /tmp/svs_ref_build.XXXXXX)
+cp "$REF_SRC"/*.cu "$REF_SRC"/*.cuh "$REF_SRC"/*.h "$REF_SRC"/bindings.cpp "$SCRATCH"/
+sed -i 's/\.type()/.scalar_type()/g' "$SCRATCH"/*.cu
+mkdir -p "$OUT" "$SCRATCH/build"
+SCRATCH="$SCRATCH" OUT="$OUT" python - <<'PY'
+import os, glob, shutil
+from torch.utils import cpp_extension
+s = os.environ["SCRATCH"]
+srcs = [os.path.join(s, "bindings.cpp")] + sorted(glob.glob(os.path.join(s, "*.cu")))
+mod = cpp_extension.load(
+    name="opticalFlow", sources=srcs, build_directory=os.path.join(s, "build"),
+    extra_cflags=["-O3"],
+    extra_cuda_cflags=["-O3", "-gencode", "arch=compute_100a,code=sm_100a"],
+    verbose=False)
+so = mod.__file__
+shutil.copy(so, os.path.join(os.environ["OUT"], os.path.basename(so)))
+open(os.path.join(os.environ["OUT"], "__init__.py"), "w").close()
+print("built", os.path.join(os.environ["OUT"], os.path.basename(so)))
+PY

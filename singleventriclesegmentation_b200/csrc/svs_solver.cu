@@ -1,0 +1,1045 @@
+// Fused batched TV-L1 solver of libsvsflow: TVL13DOpticalFlow.compute
+// (svs/modules/flow/tvl13d.py:122-255) for many independent frame pairs at once.
+//
+// Data layout in HBM (per pair and pyramid level, n = NZ*NY*NX voxels): every field is PLANAR
+// (component-major: comp c of voxel v at [c*n + v]) so that a warp's 32 consecutive x-voxels
+// read 32 consecutive elements of each component.
+//   float : I0, I1 (level images), g1 = grad I1 (3 planes)
+//   S     : D (6 planes, the symmetric anisotropic tensor s n n^T + t1 t1^T packed
+//           d00 d01 d02 d11 d12 d22), rc (rho_c), gw (warped gradient, 3 planes),
+//           u[2] (3 planes each, ping-pong), p[2] (9 planes each, ping-pong)
+// S is float, bf16 or fp16 storage; all arithmetic is float.
+//
+// Kernels per solve: blur (level 0), restrict (levels 1..L-1), and per level: prepare (grad I1
+// and D), then per warp: linearise (I1(x+u), grad I1(x+u), rho_c), then per iteration ONE
+// iterate kernel that does the dual step and the primal step of tvl13d.py:213-253 together.
+// The iterate kernel marches along z through a TX x TY column tile: for each plane it computes
+// the new dual field on the tile plus a one-voxel x/y halo (recomputed, so no grid-wide
+// dependency between the two half steps) and the new flow on the plane below. The only
+// per-iteration HBM traffic is read u, p, D, rc, gw and write u, p: 34 values per voxel.
+// The whole batched solve is captured once into a CUDA graph.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "svs_common.cuh"
+
+namespace svs {
+namespace {
+
+// ------------------------------------------------------------------------- storage conversions
+template <typename S> struct Store;
+template <> struct Store<float> {
+  static __device__ __forceinline__ float ld(const float* p) { return __ldg(p); }
+  static __device__ __forceinline__ float ld_plain(const float* p) { return *p; }
+  static __device__ __forceinline__ void st(float* p, float v) { *p = v; }
+};
+template <> struct Store<__nv_bfloat16> {
+  static __device__ __forceinline__ float ld(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
+  static __device__ __forceinline__ float ld_plain(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+  static __device__ __forceinline__ void st(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+};
+template <> struct Store<__half> {
+  static __device__ __forceinline__ float ld(const __half* p) { return __half2float(__ldg(p)); }
+  static __device__ __forceinline__ float ld_plain(const __half* p) { return __half2float(*p); }
+  static __device__ __forceinline__ void st(__half* p, float v) { *p = __float2half_rn(v); }
+};
+
+// One (pair, level) of the batch.
+struct Desc {
+  int nz, ny, nx, pad0;
+  float hz, hy, hx, pad1;
+  float lz, ly, lx, pad2;
+  long long n;
+  const float* I0;
+  const float* I1;
+  float* g1;
+  void* D;
+  void* rc;
+  void* gw;
+  void* u[2];
+  void* p[2];
+};
+
+// One CTA of the iterate kernel: a column tile [x0, x0+TX) x [y0, y0+TY) x [z0, z1).
+struct Tile {
+  int desc;
+  int x0, y0;
+  int z0z1;  // z0 | z1 << 16
+};
+
+struct IterArgs {
+  float sigma, tau, factor, wtv;
+  int src, bdry;
+};
+
+struct TileShape {
+  int tx, ty;
+};
+// The iterate-kernel tile shapes compiled into the library (id 1..N; 0 = automatic).
+constexpr TileShape kTileShapes[] = {{32, 8}, {32, 4}, {16, 8}, {64, 4}, {16, 16}, {32, 16}};
+constexpr int kNumTileShapes = sizeof(kTileShapes) / sizeof(kTileShapes[0]);
+
+// ------------------------------------------------------------------------------ small kernels
+// grid: (ceil(max voxels / 256), pairs). Desc array offset selects the level.
+
+// Gaussian pre-blur of both frames, flow_utils.py:94-112 (zero padding, (2r+1)^3 taps).
+struct BlurW {
+  float w[729];  // up to 9^3 taps (sigma < 2)
+};
+__global__ void blur_pair_kernel(const Desc* __restrict__ descs, float* const* __restrict__ raw,
+                                 int r, const __grid_constant__ BlurW W, int use_blur) {
+  const Desc d = descs[blockIdx.y];
+  const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (v >= d.n) return;
+  const float* in0 = raw[2 * blockIdx.y];
+  const float* in1 = raw[2 * blockIdx.y + 1];
+  float* out0 = const_cast<float*>(d.I0);
+  float* out1 = const_cast<float*>(d.I1);
+  if (!use_blur) {
+    out0[v] = in0[v];
+    out1[v] = in1[v];
+    return;
+  }
+  const int x = (int)(v % d.nx), y = (int)((v / d.nx) % d.ny), z = (int)(v / ((int64_t)d.nx * d.ny));
+  const int k = 2 * r + 1;
+  float a0 = 0.f, a1 = 0.f;
+  for (int a = 0; a < k; ++a) {
+    const int zz = z + a - r;
+    if (zz < 0 || zz >= d.nz) continue;
+    for (int b = 0; b < k; ++b) {
+      const int yy = y + b - r;
+      if (yy < 0 || yy >= d.ny) continue;
+      const size_t row = ((size_t)zz * d.ny + yy) * d.nx;
+      const float* wr = W.w + (a * k + b) * k;
+      for (int c = 0; c < k; ++c) {
+        const int xx = x + c - r;
+        if (xx < 0 || xx >= d.nx) continue;
+        a0 = fmaf(wr[c], __ldg(in0 + row + xx), a0);
+        a1 = fmaf(wr[c], __ldg(in1 + row + xx), a1);
+      }
+    }
+  }
+  out0[v] = a0;
+  out1[v] = a1;
+}
+
+// Restriction of I0, I1 from level l-1 (fine) to level l, prolongationOps.cu:533-559 with the
+// source coordinate (i*h_c)*L_f/L_c.
+__global__ void restrict_kernel(const Desc* __restrict__ fine, const Desc* __restrict__ coarse,
+                                int interp, int bdry) {
+  const Desc f = fine[blockIdx.y], c = coarse[blockIdx.y];
+  const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (v >= c.n) return;
+  const int x = (int)(v % c.nx), y = (int)((v / c.nx) % c.ny), z = (int)(v / ((int64_t)c.nx * c.ny));
+  const float cx = (float)x * c.hx * f.lx / c.lx;
+  const float cy = (float)y * c.hy * f.ly / c.ly;
+  const float cz = (float)z * c.hz * f.lz / c.lz;
+  FieldRef r0{f.I0, f.nz, f.ny, f.nx, 1}, r1{f.I1, f.nz, f.ny, f.nx, 1};
+  const_cast<float*>(c.I0)[v] = sample(r0, cz, cy, cx, f.hz, f.hy, f.hx, interp, bdry);
+  const_cast<float*>(c.I1)[v] = sample(r1, cz, cy, cx, f.hz, f.hy, f.hx, interp, bdry);
+}
+
+// Per-level preparation, tvl13d.py:179-192: g1 = grad I1 (differentialOps.cu:540-655), the
+// anisotropic tensor from s, n, t1 (anisotropicDifferentialOps.cu:89-141) packed as a symmetric
+// matrix, and (coarsest level only) zero u and p.
+template <typename S>
+__global__ void prepare_kernel(const Desc* __restrict__ descs, int use_aniso, float alpha,
+                               float beta, int bdry, int zero_state, int src) {
+  const Desc d = descs[blockIdx.y];
+  const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (v >= d.n) return;
+  const int x = (int)(v % d.nx), y = (int)((v / d.nx) % d.ny), z = (int)(v / ((int64_t)d.nx * d.ny));
+  const float* I = d.I1;
+  const int64_t sy = d.nx, sz = (int64_t)d.nx * d.ny;
+  const float c = I[v];
+  const float g0 = fwd_axis(x > 0 ? I[v - 1] : 0.f, c, x < d.nx - 1 ? I[v + 1] : 0.f, x, d.nx, bdry, d.hx);
+  const float g1 = fwd_axis(y > 0 ? I[v - sy] : 0.f, c, y < d.ny - 1 ? I[v + sy] : 0.f, y, d.ny, bdry, d.hy);
+  const float g2 = fwd_axis(z > 0 ? I[v - sz] : 0.f, c, z < d.nz - 1 ? I[v + sz] : 0.f, z, d.nz, bdry, d.hz);
+  d.g1[v] = g0;
+  d.g1[d.n + v] = g1;
+  d.g1[2 * d.n + v] = g2;
+  float D[6] = {1.f, 0.f, 0.f, 1.f, 0.f, 1.f};
+  if (use_aniso) {
+    const float norm = sqrtf(g0 * g0 + g1 * g1 + g2 * g2);
+    if (norm > 0.f) {
+      const float s = expf(-alpha * powf(norm, beta));
+      const float n0 = g0 / norm, n1 = g1 / norm, n2 = g2 / norm;
+      float a0, a1, a2;
+      if (n2 > 0.5f) { a0 = n2; a1 = 0.f; a2 = -n0; }
+      else { a0 = n1; a1 = -n0; a2 = 0.f; }
+      D[0] = s * n0 * n0 + a0 * a0;
+      D[1] = s * n0 * n1 + a0 * a1;
+      D[2] = s * n0 * n2 + a0 * a2;
+      D[3] = s * n1 * n1 + a1 * a1;
+      D[4] = s * n1 * n2 + a1 * a2;
+      D[5] = s * n2 * n2 + a2 * a2;
+    } else {
+      for (int i = 0; i < 6; ++i) D[i] = 0.f;
+    }
+  }
+  S* Dp = reinterpret_cast<S*>(d.D);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) Store<S>::st(Dp + i * d.n + v, D[i]);
+  if (zero_state) {
+    S* u = reinterpret_cast<S*>(d.u[src]);
+    S* p = reinterpret_cast<S*>(d.p[src]);
+    for (int i = 0; i < 3; ++i) Store<S>::st(u + i * d.n + v, 0.f);
+    for (int i = 0; i < 9; ++i) Store<S>::st(p + i * d.n + v, 0.f);
+  }
+}
+
+// Tricubic sample of four fields (I1 and the 3 planes of grad I1) at one coordinate, sharing
+// the folded indices (warpingOps.cu:572-596 and :632-660 recompute them per component).
+__device__ __forceinline__ void sample_cubic4(const float* __restrict__ I, const float* __restrict__ G,
+                                              int64_t n, int nz, int ny, int nx, float cz, float cy,
+                                              float cx, float hz, float hy, float hx, int bdry,
+                                              float out[4]) {
+  int ix, iy, iz;
+  float wx, wy, wz;
+  split_coord(cx, hx, ix, wx);
+  split_coord(cy, hy, iy, wy);
+  split_coord(cz, hz, iz, wz);
+  int xs[4], ys[4];
+#pragma unroll
+  for (int d = 0; d < 4; ++d) {
+    xs[d] = fold(ix + d - 1, nx, bdry);
+    ys[d] = fold(iy + d - 1, ny, bdry);
+  }
+  float bz[4][4];
+#pragma unroll
+  for (int dz = 0; dz < 4; ++dz) {
+    const int zz = fold(iz + dz - 1, nz, bdry);
+    float by[4][4];
+#pragma unroll
+    for (int dy = 0; dy < 4; ++dy) {
+      const int64_t row = ((int64_t)zz * ny + ys[dy]) * nx;
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        const float* F = (f == 0) ? I : G + (f - 1) * n;
+        by[f][dy] = hermite4(__ldg(F + row + xs[0]), __ldg(F + row + xs[1]), __ldg(F + row + xs[2]),
+                             __ldg(F + row + xs[3]), wx);
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < 4; ++f) bz[f][dz] = hermite4(by[f][0], by[f][1], by[f][2], by[f][3], wy);
+  }
+#pragma unroll
+  for (int f = 0; f < 4; ++f) out[f] = hermite4(bz[f][0], bz[f][1], bz[f][2], bz[f][3], wz);
+}
+
+// Per-warp linearisation, tvl13d.py:196-201: I1w = I1(x+u), gw = (grad I1)(x+u),
+// rho_c = I1w - u.gw - I0.
+template <typename S>
+__global__ void linearise_kernel(const Desc* __restrict__ descs, int src, int interp, int bdry) {
+  const Desc d = descs[blockIdx.y];
+  const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (v >= d.n) return;
+  const int x = (int)(v % d.nx), y = (int)((v / d.nx) % d.ny), z = (int)(v / ((int64_t)d.nx * d.ny));
+  const S* u = reinterpret_cast<const S*>(d.u[src]);
+  const float u0 = Store<S>::ld(u + v), u1 = Store<S>::ld(u + d.n + v), u2 = Store<S>::ld(u + 2 * d.n + v);
+  const float cx = (float)x * d.hx + u0;
+  const float cy = (float)y * d.hy + u1;
+  const float cz = (float)z * d.hz + u2;
+  float s[4];
+  if (interp == SVS_INTERPOLATE_CUBIC_HERMITESPLINE) {
+    sample_cubic4(d.I1, d.g1, d.n, d.nz, d.ny, d.nx, cz, cy, cx, d.hz, d.hy, d.hx, bdry, s);
+  } else {
+    for (int f = 0; f < 4; ++f) {
+      FieldRef r{f == 0 ? d.I1 : d.g1 + (f - 1) * d.n, d.nz, d.ny, d.nx, 1};
+      s[f] = sample(r, cz, cy, cx, d.hz, d.hy, d.hx, interp, bdry);
+    }
+  }
+  const float dot = u0 * s[1] + u1 * s[2] + u2 * s[3];
+  const float rc = s[0] - dot - d.I0[v];
+  S* gw = reinterpret_cast<S*>(d.gw);
+  Store<S>::st(reinterpret_cast<S*>(d.rc) + v, rc);
+  Store<S>::st(gw + v, s[1]);
+  Store<S>::st(gw + d.n + v, s[2]);
+  Store<S>::st(gw + 2 * d.n + v, s[3]);
+}
+
+// Coarse -> fine transfer of u (scaled by L_f/L_c per axis, tvl13d.py:151-153) and p
+// (tvl13d.py:158), prolongationOps.cu:561-625; writes the fine level's buffer 0.
+template <typename S>
+__global__ void prolong_kernel(const Desc* __restrict__ coarse, const Desc* __restrict__ fine,
+                               int src, int interp, int bdry) {
+  const Desc c = coarse[blockIdx.y], f = fine[blockIdx.y];
+  const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (v >= f.n) return;
+  const int x = (int)(v % f.nx), y = (int)((v / f.nx) % f.ny), z = (int)(v / ((int64_t)f.nx * f.ny));
+  const float cx = (float)x * f.hx * c.lx / f.lx;
+  const float cy = (float)y * f.hy * c.ly / f.ly;
+  const float cz = (float)z * f.hz * c.lz / f.lz;
+  // python float (double) ratios applied to a float32 tensor
+  const float kx = (float)((double)f.lx / (double)c.lx);
+  const float ky = (float)((double)f.ly / (double)c.ly);
+  const float kz = (float)((double)f.lz / (double)c.lz);
+  const S* uc = reinterpret_cast<const S*>(c.u[src]);
+  const S* pc = reinterpret_cast<const S*>(c.p[src]);
+  S* uf = reinterpret_cast<S*>(f.u[0]);
+  S* pf = reinterpret_cast<S*>(f.p[0]);
+  int ix, iy, iz;
+  float wx, wy, wz;
+  split_coord(cx, c.hx, ix, wx);
+  split_coord(cy, c.hy, iy, wy);
+  split_coord(cz, c.hz, iz, wz);
+  for (int comp = 0; comp < 12; ++comp) {
+    const S* F = comp < 3 ? uc + comp * c.n : pc + (comp - 3) * c.n;
+    float val;
+    if (interp == SVS_INTERPOLATE_CUBIC_HERMITESPLINE) {
+      float bz[4];
+      for (int dz = 0; dz < 4; ++dz) {
+        const int zz = fold(iz + dz - 1, c.nz, bdry);
+        float by[4];
+        for (int dy = 0; dy < 4; ++dy) {
+          const int yy = fold(iy + dy - 1, c.ny, bdry);
+          const S* row = F + ((int64_t)zz * c.ny + yy) * c.nx;
+          by[dy] = hermite4(Store<S>::ld(row + fold(ix - 1, c.nx, bdry)), Store<S>::ld(row + fold(ix, c.nx, bdry)),
+                            Store<S>::ld(row + fold(ix + 1, c.nx, bdry)), Store<S>::ld(row + fold(ix + 2, c.nx, bdry)), wx);
+        }
+        bz[dz] = hermite4(by[0], by[1], by[2], by[3], wy);
+      }
+      val = hermite4(bz[0], bz[1], bz[2], bz[3], wz);
+    } else if (interp == SVS_INTERPOLATE_LINEAR) {
+      const int x0 = fold(ix, c.nx, bdry), x1 = fold(ix + 1, c.nx, bdry);
+      const int y0 = fold(iy, c.ny, bdry), y1 = fold(iy + 1, c.ny, bdry);
+      const int z0 = fold(iz, c.nz, bdry), z1 = fold(iz + 1, c.nz, bdry);
+      auto at = [&](int zz, int yy, int xx) { return Store<S>::ld(F + ((int64_t)zz * c.ny + yy) * c.nx + xx); };
+      val = (1 - wz) * (1 - wy) * (1 - wx) * at(z0, y0, x0);
+      val += wz * (1 - wy) * (1 - wx) * at(z1, y0, x0);
+      val += (1 - wz) * (1 - wy) * wx * at(z0, y0, x1);
+      val += wz * (1 - wy) * wx * at(z1, y0, x1);
+      val += (1 - wz) * wy * (1 - wx) * at(z0, y1, x0);
+      val += wz * wy * (1 - wx) * at(z1, y1, x0);
+      val += (1 - wz) * wy * wx * at(z0, y1, x1);
+      val += wz * wy * wx * at(z1, y1, x1);
+    } else {
+      const int xx = nearest_axis(cx, c.hx, c.nx, bdry), yy = nearest_axis(cy, c.hy, c.ny, bdry),
+                zz = nearest_axis(cz, c.hz, c.nz, bdry);
+      val = Store<S>::ld(F + ((int64_t)zz * c.ny + yy) * c.nx + xx);
+    }
+    if (comp < 3) {
+      const float k = comp == 0 ? kx : (comp == 1 ? ky : kz);
+      Store<S>::st(uf + comp * f.n + v, val * k);
+    } else {
+      Store<S>::st(pf + (comp - 3) * f.n + v, val);
+    }
+  }
+}
+
+// Level 0 planar state -> the caller's AoS layouts: u [Z,Y,X,3], p [Z,Y,X,3,3].
+template <typename S>
+__global__ void finalize_kernel(const Desc* __restrict__ descs, int src, float* const* __restrict__ u_out,
+                                float* const* __restrict__ p_out) {
+  const Desc d = descs[blockIdx.y];
+  const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (v >= d.n) return;
+  const S* u = reinterpret_cast<const S*>(d.u[src]);
+  float* uo = u_out[blockIdx.y];
+  for (int c = 0; c < 3; ++c) uo[3 * v + c] = Store<S>::ld(u + c * d.n + v);
+  float* po = p_out[blockIdx.y];
+  if (po) {
+    const S* p = reinterpret_cast<const S*>(d.p[src]);
+    for (int c = 0; c < 9; ++c) po[9 * v + c] = Store<S>::ld(p + c * d.n + v);
+  }
+}
+
+// Optional warm start (num_scales == 1 only: otherwise the reference overwrites u and p,
+// tvl13d.py:150, 158): AoS caller fields -> level-0 planar buffer 0.
+template <typename S>
+__global__ void warm_start_kernel(const Desc* __restrict__ descs, const float* const* __restrict__ u_in,
+                                  const float* const* __restrict__ p_in) {
+  const Desc d = descs[blockIdx.y];
+  const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (v >= d.n) return;
+  const float* ui = u_in[blockIdx.y];
+  const float* pi = p_in[blockIdx.y];
+  S* u = reinterpret_cast<S*>(d.u[0]);
+  S* p = reinterpret_cast<S*>(d.p[0]);
+  for (int c = 0; c < 3; ++c) Store<S>::st(u + c * d.n + v, ui ? ui[3 * v + c] : 0.f);
+  for (int c = 0; c < 9; ++c) Store<S>::st(p + c * d.n + v, pi ? pi[9 * v + c] : 0.f);
+}
+
+// ----------------------------------------------------------------------------- iterate kernel
+// One primal-dual iteration (tvl13d.py:213-253) over a column tile, marching along z.
+//
+// Thread (tx, ty) of the (TX+2) x (TY+2) block owns column (x0-1+tx, y0-1+ty) of the "dual
+// region" (tile plus a one-voxel halo). At plane k the block
+//   1. publishes u(k) of its columns (and a second halo ring) to shared memory,
+//   2. computes on the dual region (minus its 4 corners) p_new(k) = proj(p + sigma D grad u)
+//      and q = D p_new, keeping the z-row of q in registers and publishing the x- and y-rows,
+//   3. on the tile interior, finishes plane k-1: div = adjoint(q) from the published rows and
+//      the registers of planes k-2 and k, then u_new(k-1) = prox_primal(u - tau div).
+// One __syncthreads per plane. Halo duals are recomputed by neighbouring tiles, so each
+// launch is independent of every other tile of the same launch (ping-pong u and p).
+template <typename S, int TX, int TY>
+__global__ void __launch_bounds__((TX + 2) * (TY + 2))
+iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, IterArgs a) {
+  constexpr int PX = TX + 2, PY = TY + 2, UX = TX + 4, UY = TY + 4;
+  constexpr int NRING = 2 * (TX + TY);
+  __shared__ float su[2][3][UY][UX];
+  __shared__ float sq[2][6][PY][PX];
+
+  const Tile T = tiles[blockIdx.x];
+  const Desc& Dg = descs[T.desc];
+  const int nz = Dg.nz, ny = Dg.ny, nx = Dg.nx;
+  const float hz = Dg.hz, hy = Dg.hy, hx = Dg.hx;
+  const int64_t n = Dg.n;
+  const int z0 = T.z0z1 & 0xffff, z1 = T.z0z1 >> 16;
+  const S* __restrict__ u_src = reinterpret_cast<const S*>(Dg.u[a.src]);
+  const S* __restrict__ p_src = reinterpret_cast<const S*>(Dg.p[a.src]);
+  S* __restrict__ u_dst = reinterpret_cast<S*>(Dg.u[a.src ^ 1]);
+  S* __restrict__ p_dst = reinterpret_cast<S*>(Dg.p[a.src ^ 1]);
+  const S* __restrict__ Dm = reinterpret_cast<const S*>(Dg.D);
+  const S* __restrict__ rcm = reinterpret_cast<const S*>(Dg.rc);
+  const S* __restrict__ gwm = reinterpret_cast<const S*>(Dg.gw);
+
+  const int tid = threadIdx.x;
+  const int tx = tid % PX, ty = tid / PX;
+  const int gx = T.x0 - 1 + tx, gy = T.y0 - 1 + ty;
+  const bool in_dom = gx >= 0 && gx < nx && gy >= 0 && gy < ny;
+  const bool corner = (tx == 0 || tx == PX - 1) && (ty == 0 || ty == PY - 1);
+  const bool dual_on = in_dom && !corner;
+  const bool interior = in_dom && tx >= 1 && tx <= TX && ty >= 1 && ty <= TY;
+  const int64_t col = (int64_t)gy * nx + gx;  // voxel index of this column at z = 0
+  const int64_t plane = (int64_t)nx * ny;
+
+  // second halo ring (u only): cells at distance 2 from the tile along x or y
+  int rx = -1, ry = -1;
+  if (tid < NRING) {
+    int r = tid;
+    if (r < TY) { rx = 0; ry = 2 + r; }
+    else if ((r -= TY) < TY) { rx = UX - 1; ry = 2 + r; }
+    else if ((r -= TY) < TX) { rx = 2 + r; ry = 0; }
+    else { r -= TX; rx = 2 + r; ry = UY - 1; }
+  }
+  const int rgx = T.x0 - 2 + rx, rgy = T.y0 - 2 + ry;
+  const bool ring_on = tid < NRING && rgx >= 0 && rgx < nx && rgy >= 0 && rgy < ny;
+  const int64_t rcol = (int64_t)rgy * nx + rgx;
+
+  const int kb = max(z0 - 1, 0), ke = min(z1, nz - 1);
+  float um[3] = {0.f, 0.f, 0.f}, uc[3] = {0.f, 0.f, 0.f}, up[3] = {0.f, 0.f, 0.f};
+  if (in_dom) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (kb >= 1) um[c] = Store<S>::ld(u_src + c * n + (kb - 1) * plane + col);
+      uc[c] = Store<S>::ld(u_src + c * n + kb * plane + col);
+      if (kb + 1 < nz) up[c] = Store<S>::ld(u_src + c * n + (kb + 1) * plane + col);
+    }
+  }
+  float qzmm[3] = {0.f, 0.f, 0.f}, qzm[3] = {0.f, 0.f, 0.f}, qzc[3] = {0.f, 0.f, 0.f};
+  const float sigma = a.sigma, tau = a.tau, factor = a.factor, wtv = a.wtv;
+  const int bdry = a.bdry;
+
+  for (int k = kb; k <= ke; ++k) {
+    const int slot = k & 1;
+    // --- loads for this step (issued before the barrier)
+    float pk[9], Dk[6];
+    if (dual_on) {
+      const int64_t o = k * plane + col;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) pk[c] = Store<S>::ld(p_src + c * n + o);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) Dk[c] = Store<S>::ld(Dm + c * n + o);
+    }
+    const int j = k - 1;  // plane finished in this step
+    const bool primal_on = interior && j >= z0 && j < z1;
+    float rcj = 0.f, gj[3] = {0.f, 0.f, 0.f};
+    if (primal_on) {
+      const int64_t o = j * plane + col;
+      rcj = Store<S>::ld(rcm + o);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) gj[c] = Store<S>::ld(gwm + c * n + o);
+    }
+    // --- 1. publish u(k)
+    if (in_dom) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) su[slot][c][ty + 1][tx + 1] = uc[c];
+    }
+    if (ring_on) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) su[slot][c][ry][rx] = Store<S>::ld(u_src + c * n + k * plane + rcol);
+    }
+    __syncthreads();
+    // --- 2. dual step at plane k
+    if (dual_on) {
+      float pn[9];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float ex = fwd_axis(su[slot][c][ty + 1][tx], uc[c], su[slot][c][ty + 1][tx + 2], gx, nx, bdry, hx);
+        const float ey = fwd_axis(su[slot][c][ty][tx + 1], uc[c], su[slot][c][ty + 2][tx + 1], gy, ny, bdry, hy);
+        const float ez = fwd_axis(um[c], uc[c], up[c], k, nz, bdry, hz);
+        const float dz0 = Dk[0] * ex + Dk[1] * ey + Dk[2] * ez;
+        const float dz1 = Dk[1] * ex + Dk[3] * ey + Dk[4] * ez;
+        const float dz2 = Dk[2] * ex + Dk[4] * ey + Dk[5] * ez;
+        const float v0 = pk[3 * c] + sigma * dz0;
+        const float v1 = pk[3 * c + 1] + sigma * dz1;
+        const float v2 = pk[3 * c + 2] + sigma * dz2;
+        // projection onto the ball of radius weight_tv, opticalFlowOps.cu:193-206
+        const float den = fmaxf(1.0f, sqrtf(v0 * v0 + v1 * v1 + v2 * v2) / wtv);
+        if (wtv > 0.f) {
+          pn[3 * c] = v0 / den;
+          pn[3 * c + 1] = v1 / den;
+          pn[3 * c + 2] = v2 / den;
+        } else {  // tvl13d.py:223-224
+          pn[3 * c] = pn[3 * c + 1] = pn[3 * c + 2] = 0.f;
+        }
+      }
+      if (interior && k >= z0 && k < z1) {
+        const int64_t o = k * plane + col;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) Store<S>::st(p_dst + c * n + o, pn[c]);
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float q0 = Dk[0] * pn[3 * c] + Dk[1] * pn[3 * c + 1] + Dk[2] * pn[3 * c + 2];
+        const float q1 = Dk[1] * pn[3 * c] + Dk[3] * pn[3 * c + 1] + Dk[4] * pn[3 * c + 2];
+        const float q2 = Dk[2] * pn[3 * c] + Dk[4] * pn[3 * c + 1] + Dk[5] * pn[3 * c + 2];
+        sq[slot][c][ty][tx] = q0;
+        sq[slot][3 + c][ty][tx] = q1;
+        qzc[c] = q2;
+      }
+    }
+    // --- 3. primal step at plane j = k-1 (its x/y rows were published in the previous step)
+    if (primal_on) {
+      const int ps = slot ^ 1;
+      float un[3];
+      const float rho = rcj + (um[0] * gj[0] + um[1] * gj[1] + um[2] * gj[2]);
+      const float g2s = gj[0] * gj[0] + gj[1] * gj[1] + gj[2] * gj[2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float ax = adj_axis(sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1], gx, nx, bdry);
+        const float ay = adj_axis(sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx], gy, ny, bdry);
+        const float az = adj_axis(qzmm[c], qzm[c], qzc[c], j, nz, bdry);
+        const float div = (ax / hx + ay / hy) + az / hz;
+        un[c] = um[c] - tau * div;
+      }
+      // L1 data-term shrinkage, opticalFlowOps.cu:140-171
+      if (rho < -factor * g2s) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) un[c] += factor * gj[c];
+      } else if (rho > factor * g2s) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) un[c] += -factor * gj[c];
+      } else if (g2s > 1e-10f) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) un[c] += -rho * gj[c] / g2s;
+      }
+      const int64_t o = j * plane + col;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) Store<S>::st(u_dst + c * n + o, un[c]);
+    }
+    // --- roll the z window
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      qzmm[c] = qzm[c];
+      qzm[c] = qzc[c];
+      um[c] = uc[c];
+      uc[c] = up[c];
+      up[c] = 0.f;
+    }
+    if (in_dom && k + 2 < nz) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) up[c] = Store<S>::ld(u_src + c * n + (k + 2) * plane + col);
+    }
+  }
+  // last plane of the volume: its dual rows were published in the final step
+  if (z1 >= nz) {
+    __syncthreads();
+    const int j = nz - 1;
+    if (interior && j >= z0) {
+      const int ps = j & 1;
+      const int64_t o = j * plane + col;
+      const float rcj = Store<S>::ld(rcm + o);
+      float gj[3], un[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) gj[c] = Store<S>::ld(gwm + c * n + o);
+      const float rho = rcj + (um[0] * gj[0] + um[1] * gj[1] + um[2] * gj[2]);
+      const float g2s = gj[0] * gj[0] + gj[1] * gj[1] + gj[2] * gj[2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float ax = adj_axis(sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1], gx, nx, bdry);
+        const float ay = adj_axis(sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx], gy, ny, bdry);
+        const float az = adj_axis(qzmm[c], qzm[c], 0.f, j, nz, bdry);
+        const float div = (ax / hx + ay / hy) + az / hz;
+        un[c] = um[c] - tau * div;
+      }
+      if (rho < -factor * g2s) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) un[c] += factor * gj[c];
+      } else if (rho > factor * g2s) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) un[c] += -factor * gj[c];
+      } else if (g2s > 1e-10f) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) un[c] += -rho * gj[c] / g2s;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) Store<S>::st(u_dst + c * n + o, un[c]);
+    }
+  }
+}
+
+}  // namespace
+}  // namespace svs
+
+// =============================================================================================
+// Host side: plan (device state + tile lists), the enqueue sequence, CUDA-graph capture.
+// =============================================================================================
+struct svs_plan {
+  svs_tvl1_params prm{};
+  int num_pairs = 0;
+  int levels = 0;
+  std::vector<int> dims;                   // level-0 dims, 3 per pair
+  std::vector<svs::Desc> h_descs;          // [levels][pairs]
+  svs::Desc* d_descs = nullptr;
+  std::vector<std::vector<svs::Tile>> h_tiles;  // per level
+  std::vector<svs::Tile*> d_tiles;
+  int tile_id = 0;                         // 0 = automatic
+  int tiles_built_for = -1;
+  void* arena = nullptr;
+  size_t arena_bytes = 0;
+  float** d_raw = nullptr;                 // [2*pairs] raw input frames (device)
+  float** d_uout = nullptr;                // [pairs] AoS u results
+  float** d_pout = nullptr;                // [pairs] AoS p results (or null entries)
+  float** d_umed = nullptr;                // [pairs] median outputs
+  const float** d_uinit = nullptr;         // [pairs] warm start (num_scales == 1)
+  const float** d_pinit = nullptr;
+  std::vector<float*> raw, uout, pout, umed;
+  std::vector<const float*> uinit, pinit;
+  std::vector<float> sig_sched, tau_sched;  // per iteration inside one warp
+  svs::BlurW blur{};
+  int blur_r = 0;
+  bool want_p = false;
+  bool warm = false;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t graph_kernels = 0;
+  int graph_tile = -1;
+  bool graph_warm = false;
+  bool graph_want_p = false;
+};
+
+namespace svs {
+namespace {
+
+size_t storage_bytes(int storage) { return storage == SVS_STORAGE_F32 ? 4 : 2; }
+
+// Automatic tile choice for a level: 32x8 columns; z is split into chunks only when the batch
+// has too few column tiles to fill the GPU (single small pairs).
+int auto_tile(const svs_plan& P, int level) {
+  (void)P;
+  (void)level;
+  return 1;
+}
+
+void build_tiles(svs_plan& P, int tile_id) {
+  P.h_tiles.assign(P.levels, {});
+  for (int l = 0; l < P.levels; ++l) {
+    const int tid = tile_id > 0 ? tile_id : auto_tile(P, l);
+    const TileShape ts = kTileShapes[tid - 1];
+    long long xy_tiles = 0;
+    for (int i = 0; i < P.num_pairs; ++i) {
+      const Desc& d = P.h_descs[(size_t)l * P.num_pairs + i];
+      xy_tiles += (long long)ceil_div(d.nx, ts.tx) * ceil_div(d.ny, ts.ty);
+    }
+    const long long target = 148LL * 4;
+    for (int i = 0; i < P.num_pairs; ++i) {
+      const Desc& d = P.h_descs[(size_t)l * P.num_pairs + i];
+      int chunks = 1;
+      if (xy_tiles < target) chunks = (int)std::min<long long>((target + xy_tiles - 1) / xy_tiles, std::max(1, d.nz / 8));
+      const int zc = (d.nz + chunks - 1) / chunks;
+      for (int z0 = 0; z0 < d.nz; z0 += zc)
+        for (int y0 = 0; y0 < d.ny; y0 += ts.ty)
+          for (int x0 = 0; x0 < d.nx; x0 += ts.tx) {
+            const int z1 = std::min(d.nz, z0 + zc);
+            P.h_tiles[l].push_back(Tile{l * P.num_pairs + i, x0, y0, z0 | (z1 << 16)});
+          }
+    }
+  }
+}
+
+svs_status upload_tiles(svs_plan& P) {
+  for (auto* p : P.d_tiles) cudaFree(p);
+  P.d_tiles.assign(P.levels, nullptr);
+  for (int l = 0; l < P.levels; ++l) {
+    const size_t bytes = P.h_tiles[l].size() * sizeof(Tile);
+    svs_status st = check_cuda(cudaMalloc(&P.d_tiles[l], bytes), "tile list");
+    if (st) return st;
+    st = check_cuda(cudaMemcpy(P.d_tiles[l], P.h_tiles[l].data(), bytes, cudaMemcpyHostToDevice), "tile list");
+    if (st) return st;
+  }
+  return SVS_OK;
+}
+
+template <typename S, int TX, int TY>
+void launch_iter(const svs_plan& P, int level, const IterArgs& a, cudaStream_t s) {
+  const unsigned nt = (unsigned)P.h_tiles[level].size();
+  iterate_kernel<S, TX, TY><<<nt, (TX + 2) * (TY + 2), 0, s>>>(P.d_tiles[level], P.d_descs, a);
+}
+
+template <typename S>
+void launch_iter_shape(const svs_plan& P, int level, int tid, const IterArgs& a, cudaStream_t s) {
+  switch (tid) {
+    case 1: launch_iter<S, 32, 8>(P, level, a, s); break;
+    case 2: launch_iter<S, 32, 4>(P, level, a, s); break;
+    case 3: launch_iter<S, 16, 8>(P, level, a, s); break;
+    case 4: launch_iter<S, 64, 4>(P, level, a, s); break;
+    case 5: launch_iter<S, 16, 16>(P, level, a, s); break;
+    default: launch_iter<S, 32, 16>(P, level, a, s); break;
+  }
+}
+
+long long max_voxels(const svs_plan& P, int level) {
+  long long m = 0;
+  for (int i = 0; i < P.num_pairs; ++i) m = std::max(m, P.h_descs[(size_t)level * P.num_pairs + i].n);
+  return m;
+}
+
+// The whole batched solve as a sequence of launches on stream s. Returns the number of kernel
+// launches issued (for the launch counter) or -1 after a launch error.
+template <typename S>
+long long enqueue_solve(svs_plan& P, cudaStream_t s) {
+  const svs_tvl1_params& q = P.prm;
+  const int L = P.levels, np = P.num_pairs;
+  long long launches = 0;
+  auto grid = [&](int level) { return dim3(ceil_div(max_voxels(P, level), 256), np); };
+  const Desc* D = P.d_descs;
+  blur_pair_kernel<<<grid(0), 256, 0, s>>>(D, P.d_raw, P.blur_r, P.blur, q.use_gaussian_blur);
+  ++launches;
+  for (int l = 1; l < L; ++l) {
+    restrict_kernel<<<grid(l), 256, 0, s>>>(D + (size_t)(l - 1) * np, D + (size_t)l * np, q.interpolation, q.boundary);
+    ++launches;
+  }
+  if (P.warm && L == 1) {
+    warm_start_kernel<S><<<grid(0), 256, 0, s>>>(D, P.d_uinit, P.d_pinit);
+    ++launches;
+  }
+  int cur = 0;
+  const float wm = q.weight_matching;
+  for (int l = L - 1; l >= 0; --l) {
+    const int zero = (l == L - 1) && !(P.warm && L == 1);
+    prepare_kernel<S><<<grid(l), 256, 0, s>>>(D + (size_t)l * np, q.use_anisotropic_diff, q.alpha, q.beta, q.boundary, zero, cur);
+    ++launches;
+    const int tid = P.tile_id > 0 ? P.tile_id : auto_tile(P, l);
+    for (int w = 0; w < q.max_warps; ++w) {
+      linearise_kernel<S><<<grid(l), 256, 0, s>>>(D + (size_t)l * np, cur, q.interpolation, q.boundary);
+      ++launches;
+      for (int it = 0; it < q.max_outer_iterations; ++it) {
+        IterArgs a;
+        a.sigma = P.sig_sched[it];
+        a.tau = P.tau_sched[it];
+        a.factor = a.tau * wm;  // opticalFlowOps.cu:440
+        a.wtv = q.weight_tv;
+        a.src = cur;
+        a.bdry = q.boundary;
+        launch_iter_shape<S>(P, l, tid, a, s);
+        ++launches;
+        cur ^= 1;
+      }
+    }
+    if (l > 0) {
+      prolong_kernel<S><<<grid(l - 1), 256, 0, s>>>(D + (size_t)l * np, D + (size_t)(l - 1) * np, cur, q.interpolation, q.boundary);
+      ++launches;
+      cur = 0;
+    }
+  }
+  float** uo = q.median_kernel > 1 ? P.d_umed : P.d_uout;
+  finalize_kernel<S><<<grid(0), 256, 0, s>>>(D, cur, uo, P.d_pout);
+  ++launches;
+  if (cudaPeekAtLastError() != cudaSuccess) return -1;
+  if (q.median_kernel > 1) {
+    for (int i = 0; i < np; ++i) {
+      const Desc& d = P.h_descs[i];
+      if (svs_median3d(P.umed[i], d.nz, d.ny, d.nx, 3, q.median_kernel, P.uout[i], s) != SVS_OK) return -1;
+      ++launches;
+    }
+  }
+  return launches;
+}
+
+long long enqueue(svs_plan& P, cudaStream_t s) {
+  if (P.prm.storage == SVS_STORAGE_BF16) return enqueue_solve<__nv_bfloat16>(P, s);
+  if (P.prm.storage == SVS_STORAGE_F16) return enqueue_solve<__half>(P, s);
+  return enqueue_solve<float>(P, s);
+}
+
+template <typename T> T* carve(char*& cur, size_t count) {
+  T* p = reinterpret_cast<T*>(cur);
+  cur += (count * sizeof(T) + 255) / 256 * 256;
+  return p;
+}
+
+}  // namespace
+}  // namespace svs
+
+using namespace svs;
+
+extern "C" {
+
+int svs_tvl1_num_tiles(void) { return kNumTileShapes; }
+
+svs_status svs_tvl1_plan_create(const svs_tvl1_params* prm, int num_pairs, const int* dims,
+                                svs_plan** out) {
+  SVS_REQUIRE(prm && dims && out, "svs_tvl1_plan_create: null pointer");
+  SVS_REQUIRE(num_pairs > 0, "svs_tvl1_plan_create: num_pairs must be positive");
+  SVS_REQUIRE(prm->num_scales >= 1 && prm->num_scales <= 8, "svs_tvl1_plan_create: num_scales out of range");
+  SVS_REQUIRE(prm->max_warps >= 0 && prm->max_outer_iterations >= 0, "svs_tvl1_plan_create: negative iteration count");
+  SVS_REQUIRE(prm->primaldual_algorithm_type == 1 || prm->primaldual_algorithm_type == 2,
+              "svs_tvl1_plan_create: primaldual_algorithm_type must be 1 or 2");
+  SVS_REQUIRE(prm->boundary >= 0 && prm->boundary <= 2, "svs_tvl1_plan_create: bad boundary type");
+  SVS_REQUIRE(prm->interpolation >= 0 && prm->interpolation <= 2, "svs_tvl1_plan_create: bad interpolation type");
+  SVS_REQUIRE(prm->storage >= 0 && prm->storage <= 2, "svs_tvl1_plan_create: bad storage type");
+  SVS_REQUIRE(prm->weight_tv >= 0.f, "svs_tvl1_plan_create: weight_tv must be >= 0");
+  SVS_REQUIRE(prm->median_kernel == 0 || prm->median_kernel == 1 || prm->median_kernel == 3 ||
+                  prm->median_kernel == 5 || prm->median_kernel == 7,
+              "svs_tvl1_plan_create: median kernel must be 0, 1, 3, 5 or 7");
+  svs_plan* P = new svs_plan();
+  P->prm = *prm;
+  P->num_pairs = num_pairs;
+  P->levels = prm->num_scales;
+  P->dims.assign(dims, dims + 3 * num_pairs);
+  // mesh sizes per level (tvl13d.py:91-99, ceil halving) and spacings (coreDefines.h:72-75)
+  P->h_descs.resize((size_t)P->levels * num_pairs);
+  size_t bytes = 0;
+  const size_t sb = storage_bytes(prm->storage);
+  for (int i = 0; i < num_pairs; ++i) {
+    int nz = dims[3 * i], ny = dims[3 * i + 1], nx = dims[3 * i + 2];
+    if (nz >= 65535 || ny >= 65535 || nx >= 65535) { delete P; return fail(SVS_ERR_INVALID_ARG, "svs_tvl1_plan_create: volume dimension too large"); }
+    for (int l = 0; l < P->levels; ++l) {
+      if (l > 0) { nz = (nz + 1) / 2; ny = (ny + 1) / 2; nx = (nx + 1) / 2; }
+      if (nz < 3 || ny < 3 || nx < 3) {
+        delete P;
+        return fail(SVS_ERR_INVALID_ARG, "svs_tvl1_plan_create: every pyramid level needs at least 3 nodes per axis");
+      }
+      Desc& d = P->h_descs[(size_t)l * num_pairs + i];
+      std::memset(&d, 0, sizeof(d));
+      d.nz = nz; d.ny = ny; d.nx = nx;
+      d.n = (long long)nz * ny * nx;
+      if (prm->length_type == 0) { d.lz = (float)(nz - 1); d.ly = (float)(ny - 1); d.lx = (float)(nx - 1); }
+      else { d.lz = prm->length_z; d.ly = prm->length_y; d.lx = prm->length_x; }
+      d.hz = d.lz / (float)(nz - 1); d.hy = d.ly / (float)(ny - 1); d.hx = d.lx / (float)(nx - 1);
+      const size_t n = (size_t)d.n;
+      bytes += 5 * ((n * 4 + 255) / 256 * 256);           // I0, I1, g1 (3 planes)
+      bytes += (6 + 1 + 3 + 6 + 18) * ((n * sb + 255) / 256 * 256) + 34 * 256;
+      if (l == 0) bytes += (2 + 3 + 3 + 9) * ((n * 4 + 255) / 256 * 256);  // raw x2, uout, umed, pout
+    }
+  }
+  bytes += 4096;
+  svs_status st = check_cuda(cudaMalloc(&P->arena, bytes), "svs_tvl1_plan_create: device state");
+  if (st) { delete P; return st; }
+  P->arena_bytes = bytes;
+  char* cur = reinterpret_cast<char*>(P->arena);
+  P->raw.resize(2 * num_pairs); P->uout.resize(num_pairs); P->pout.resize(num_pairs); P->umed.resize(num_pairs);
+  P->uinit.assign(num_pairs, nullptr); P->pinit.assign(num_pairs, nullptr);
+  for (int l = 0; l < P->levels; ++l)
+    for (int i = 0; i < num_pairs; ++i) {
+      Desc& d = P->h_descs[(size_t)l * num_pairs + i];
+      const size_t n = (size_t)d.n;
+      d.I0 = carve<float>(cur, n);
+      d.I1 = carve<float>(cur, n);
+      d.g1 = carve<float>(cur, 3 * n);
+      d.D = carve<char>(cur, 6 * n * sb);
+      d.rc = carve<char>(cur, n * sb);
+      d.gw = carve<char>(cur, 3 * n * sb);
+      d.u[0] = carve<char>(cur, 3 * n * sb);
+      d.u[1] = carve<char>(cur, 3 * n * sb);
+      d.p[0] = carve<char>(cur, 9 * n * sb);
+      d.p[1] = carve<char>(cur, 9 * n * sb);
+      if (l == 0) {
+        P->raw[2 * i] = carve<float>(cur, n);
+        P->raw[2 * i + 1] = carve<float>(cur, n);
+        P->uout[i] = carve<float>(cur, 3 * n);
+        P->umed[i] = carve<float>(cur, 3 * n);
+        P->pout[i] = carve<float>(cur, 9 * n);
+      }
+    }
+  auto upload = [&](void** dptr, const void* src, size_t sz) -> svs_status {
+    svs_status s2 = check_cuda(cudaMalloc(dptr, sz), "svs_tvl1_plan_create");
+    if (s2) return s2;
+    return check_cuda(cudaMemcpy(*dptr, src, sz, cudaMemcpyHostToDevice), "svs_tvl1_plan_create");
+  };
+  st = upload((void**)&P->d_descs, P->h_descs.data(), P->h_descs.size() * sizeof(Desc));
+  if (!st) st = upload((void**)&P->d_raw, P->raw.data(), P->raw.size() * sizeof(float*));
+  if (!st) st = upload((void**)&P->d_uout, P->uout.data(), P->uout.size() * sizeof(float*));
+  if (!st) st = upload((void**)&P->d_umed, P->umed.data(), P->umed.size() * sizeof(float*));
+  std::vector<float*> nop(num_pairs, nullptr);
+  if (!st) st = upload((void**)&P->d_pout, nop.data(), nop.size() * sizeof(float*));
+  if (!st) st = upload((void**)&P->d_uinit, P->uinit.data(), P->uinit.size() * sizeof(float*));
+  if (!st) st = upload((void**)&P->d_pinit, P->pinit.data(), P->pinit.size() * sizeof(float*));
+  if (st) { svs_tvl1_plan_destroy(P); return st; }
+  // step-size schedule within a warp (tvl13d.py:208-211 reset, :240-249 update, host float64),
+  // each value rounded to float as torch and pybind do.
+  {
+    double sg = prm->sigma, ta = prm->tau;
+    for (int it = 0; it < prm->max_outer_iterations; ++it) {
+      P->sig_sched.push_back((float)sg);
+      P->tau_sched.push_back((float)ta);
+      if (prm->primaldual_algorithm_type == 2) {
+        const double th = 1.0 / std::sqrt(1.0 + 2.0 * prm->gamma * ta);
+        ta *= th;
+        sg /= th;
+      }
+    }
+  }
+  // Gaussian kernel weights, flow_utils.py:74-91 and :106-107, in float32
+  if (prm->use_gaussian_blur) {
+    const double sgm = prm->gaussian_blur_sigma;
+    int ks = (int)(sgm * 5);
+    if (ks % 2 == 0) ks += 1;
+    if (ks > 9 || ks < 1) { svs_tvl1_plan_destroy(P); return fail(SVS_ERR_INVALID_ARG, "svs_tvl1_plan_create: gaussian_blur_sigma out of range (kernel size <= 9)"); }
+    // torch.linspace(-ks//2, ks//2 + 1, ks) with Python floor division
+    const int lo = -((ks + 1) / 2), hi = ks / 2 + 1;
+    std::vector<float> t(ks), g(ks), k1(ks);
+    for (int i = 0; i < ks; ++i) t[i] = (ks == 1) ? (float)lo : (float)(lo + (double)(hi - lo) * i / (ks - 1));
+    float gs = 0.f;
+    for (int i = 0; i < ks; ++i) {
+      const float a = t[i] / (float)sgm;
+      g[i] = std::exp(-(a * a) / 2.0f);
+      gs += g[i];
+    }
+    for (int i = 0; i < ks; ++i) k1[i] = g[i] / gs;
+    float tot = 0.f;
+    std::vector<float> k3((size_t)ks * ks * ks);
+    for (int a = 0; a < ks; ++a)
+      for (int b = 0; b < ks; ++b)
+        for (int c = 0; c < ks; ++c) { k3[(a * ks + b) * ks + c] = k1[a] * k1[b] * k1[c]; tot += k3[(a * ks + b) * ks + c]; }
+    for (size_t i = 0; i < k3.size(); ++i) P->blur.w[i] = k3[i] / tot;
+    P->blur_r = ks / 2;
+  }
+  st = check_cuda(cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking), "svs_tvl1_plan_create");
+  if (st) { svs_tvl1_plan_destroy(P); return st; }
+  *out = P;
+  return SVS_OK;
+}
+
+svs_status svs_tvl1_plan_destroy(svs_plan* P) {
+  if (!P) return SVS_OK;
+  if (P->exec) cudaGraphExecDestroy(P->exec);
+  if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
+  for (auto* t : P->d_tiles) cudaFree(t);
+  cudaFree(P->d_descs); cudaFree(P->d_raw); cudaFree(P->d_uout); cudaFree(P->d_umed);
+  cudaFree(P->d_pout); cudaFree(P->d_uinit); cudaFree(P->d_pinit);
+  cudaFree(P->arena);
+  delete P;
+  return SVS_OK;
+}
+
+size_t svs_tvl1_plan_device_bytes(const svs_plan* P) { return P ? P->arena_bytes : 0; }
+
+svs_status svs_tvl1_plan_set_tile(svs_plan* P, int tile_id) {
+  SVS_REQUIRE(P, "svs_tvl1_plan_set_tile: null plan");
+  SVS_REQUIRE(tile_id >= 0 && tile_id <= kNumTileShapes, "svs_tvl1_plan_set_tile: unknown tile id");
+  P->tile_id = tile_id;
+  return SVS_OK;
+}
+
+svs_status svs_tvl1_solve_batch(svs_plan* P, const svs_pair_desc* pairs, int num_pairs,
+                                svs_stream_t stream) {
+  SVS_REQUIRE(P && pairs, "svs_tvl1_solve_batch: null pointer");
+  SVS_REQUIRE(num_pairs == P->num_pairs, "svs_tvl1_solve_batch: pair count differs from the plan");
+  bool want_p = false, warm = false;
+  for (int i = 0; i < num_pairs; ++i) {
+    const svs_pair_desc& q = pairs[i];
+    SVS_REQUIRE(q.I0 && q.I1 && q.u_out, "svs_tvl1_solve_batch: null frame or output pointer");
+    SVS_REQUIRE(q.nz == P->dims[3 * i] && q.ny == P->dims[3 * i + 1] && q.nx == P->dims[3 * i + 2],
+                "svs_tvl1_solve_batch: pair sizes differ from the plan");
+    want_p |= q.p_out != nullptr;
+    warm |= (q.u_init != nullptr || q.p_init != nullptr);
+  }
+  warm = warm && P->levels == 1;
+  cudaStream_t s = stream;
+  svs_status st = SVS_OK;
+  // inputs -> plan buffers (one copy each)
+  for (int i = 0; i < num_pairs && !st; ++i) {
+    const size_t b = (size_t)P->h_descs[i].n * sizeof(float);
+    st = check_cuda(cudaMemcpyAsync(P->raw[2 * i], pairs[i].I0, b, cudaMemcpyDeviceToDevice, s), "solve: input copy");
+    if (!st) st = check_cuda(cudaMemcpyAsync(P->raw[2 * i + 1], pairs[i].I1, b, cudaMemcpyDeviceToDevice, s), "solve: input copy");
+  }
+  if (st) return st;
+  if (warm) {
+    for (int i = 0; i < num_pairs; ++i) { P->uinit[i] = pairs[i].u_init; P->pinit[i] = pairs[i].p_init; }
+    st = check_cuda(cudaMemcpyAsync(P->d_uinit, P->uinit.data(), num_pairs * sizeof(float*), cudaMemcpyHostToDevice, s), "solve");
+    if (!st) st = check_cuda(cudaMemcpyAsync(P->d_pinit, P->pinit.data(), num_pairs * sizeof(float*), cudaMemcpyHostToDevice, s), "solve");
+    if (!st) st = check_cuda(cudaStreamSynchronize(s), "solve");
+    if (st) return st;
+  }
+  if (want_p != P->want_p) {
+    std::vector<float*> po(num_pairs, nullptr);
+    if (want_p) po = P->pout;
+    st = check_cuda(cudaMemcpy(P->d_pout, po.data(), num_pairs * sizeof(float*), cudaMemcpyHostToDevice), "solve");
+    if (st) return st;
+    P->want_p = want_p;
+  }
+  P->warm = warm;
+  if (P->tiles_built_for != P->tile_id) {
+    build_tiles(*P, P->tile_id);
+    st = upload_tiles(*P);
+    if (st) return st;
+    P->tiles_built_for = P->tile_id;
+  }
+  // the graph: captured once per (tile, warm start, want_p) configuration
+  if (!P->exec || P->graph_tile != P->tile_id || P->graph_warm != warm || P->graph_want_p != want_p) {
+    if (P->exec) { cudaGraphExecDestroy(P->exec); P->exec = nullptr; }
+    cudaGraph_t g = nullptr;
+    st = check_cuda(cudaStreamBeginCapture(P->cap_stream, cudaStreamCaptureModeThreadLocal), "solve: capture");
+    if (st) return st;
+    const long long nl = enqueue(*P, P->cap_stream);
+    const cudaError_t ce = cudaStreamEndCapture(P->cap_stream, &g);
+    if (nl < 0) { if (g) cudaGraphDestroy(g); return fail(SVS_ERR_LAUNCH, std::string("solve: launch failed during capture: ") + cudaGetErrorString(cudaGetLastError())); }
+    st = check_cuda(ce, "solve: end capture");
+    if (st) return st;
+    st = check_cuda(cudaGraphInstantiate(&P->exec, g, 0), "solve: graph instantiate");
+    cudaGraphDestroy(g);
+    if (st) return st;
+    P->graph_kernels = (uint64_t)nl;
+    P->graph_tile = P->tile_id;
+    P->graph_warm = warm;
+    P->graph_want_p = want_p;
+  }
+  st = check_cuda(cudaGraphLaunch(P->exec, s), "solve: graph launch");
+  if (st) return st;
+  count_launches(P->graph_kernels);
+  for (int i = 0; i < num_pairs && !st; ++i) {
+    const size_t n = (size_t)P->h_descs[i].n;
+    st = check_cuda(cudaMemcpyAsync(pairs[i].u_out, P->uout[i], 3 * n * sizeof(float), cudaMemcpyDeviceToDevice, s), "solve: output copy");
+    if (!st && pairs[i].p_out)
+      st = check_cuda(cudaMemcpyAsync(pairs[i].p_out, P->pout[i], 9 * n * sizeof(float), cudaMemcpyDeviceToDevice, s), "solve: output copy");
+  }
+  return st;
+}
+
+svs_status svs_tvl1_bench_iterations(svs_plan* P, int level, int count, svs_stream_t stream) {
+  SVS_REQUIRE(P, "svs_tvl1_bench_iterations: null plan");
+  SVS_REQUIRE(level >= 0 && level < P->levels, "svs_tvl1_bench_iterations: bad level");
+  SVS_REQUIRE(count >= 0, "svs_tvl1_bench_iterations: bad count");
+  SVS_REQUIRE(P->tiles_built_for == P->tile_id, "svs_tvl1_bench_iterations: run a solve first");
+  const int tid = P->tile_id > 0 ? P->tile_id : auto_tile(*P, level);
+  int cur = 0;
+  for (int i = 0; i < count; ++i) {
+    IterArgs a;
+    const int it = P->prm.max_outer_iterations > 0 ? i % P->prm.max_outer_iterations : 0;
+    a.sigma = P->sig_sched.empty() ? 0.5f : P->sig_sched[it];
+    a.tau = P->tau_sched.empty() ? 0.5f : P->tau_sched[it];
+    a.factor = a.tau * P->prm.weight_matching;
+    a.wtv = P->prm.weight_tv;
+    a.src = cur;
+    a.bdry = P->prm.boundary;
+    if (P->prm.storage == SVS_STORAGE_BF16) launch_iter_shape<__nv_bfloat16>(*P, level, tid, a, stream);
+    else if (P->prm.storage == SVS_STORAGE_F16) launch_iter_shape<__half>(*P, level, tid, a, stream);
+    else launch_iter_shape<float>(*P, level, tid, a, stream);
+    cur ^= 1;
+  }
+  return check_launch("svs_tvl1_bench_iterations", (uint64_t)count);
+}
+
+uint64_t svs_tvl1_plan_graph_kernels(const svs_plan* P) { return P ? P->graph_kernels : 0; }
+
+}  // extern "C"

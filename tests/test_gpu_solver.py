@@ -1,0 +1,150 @@
+"""Fused batched solver parity: the CUDA path (C ABI svs_tvl1_solve_batch through
+TVL13DOpticalFlow) against the oracle's restatement of tvl13d.py, the plain per-operator form,
+and itself (batch invariance, tile invariance, graph reuse).
+
+Tolerance (float32 arithmetic): mean end-point error <= 0.05 voxel against the oracle, the bar
+the fused path must meet; the measured errors are far below it and are also bounded tightly."""
+import numpy as np
+import pytest
+import torch
+
+from singleventriclesegmentation_b200 import synthetic
+from singleventriclesegmentation_b200.tvl13d import TVL13DOpticalFlow
+
+pytestmark = pytest.mark.gpu
+
+EPE_TOL = 0.05
+
+
+def epe(a, b):
+    return np.sqrt(((np.asarray(a, np.float64) - np.asarray(b, np.float64)) ** 2).sum(-1))
+
+
+def make_solver(oracle_params=None, storage="f32", **over):
+    from oracle.oracle import SolverParams
+    P = oracle_params or SolverParams(**over)
+    return TVL13DOpticalFlow(P.num_scales, P.max_warps, P.max_outer_iterations, P.weight_matching, P.weight_tv,
+                             P.primaldual_algorithm_type, P.primaldual_algorithm_params, P.use_anisotropic_diff,
+                             P.anisotropic_diff_params, P.use_gaussian_blur, P.gaussian_blur_sigma,
+                             P.interpolation_type, P.boundary_type, P.length_type, P.length,
+                             torch.device("cuda"), storage=storage), P
+
+
+def T(a):
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device="cuda")
+
+
+@pytest.fixture(scope="module")
+def pair24():
+    return synthetic.frame_pair((24, 24, 24), seed=7)
+
+
+def test_fused_matches_oracle_default_config(cuda, oracle, pair24):
+    I0, I1, _ = pair24
+    solver, P = make_solver()
+    u, p = solver.compute(T(I0), T(I1), None, None)
+    uo, po = oracle.tvl1_compute(I0, I1, P, dtype=np.float32)
+    e = epe(u.cpu().numpy(), uo)
+    assert e.mean() <= EPE_TOL
+    assert e.mean() < 5e-3 and e.max() < 0.1, (e.mean(), e.max())
+    assert np.abs(p.cpu().numpy() - po).max() < 0.02
+
+
+def test_fused_matches_fp64_oracle(cuda, oracle, pair24):
+    I0, I1, _ = pair24
+    solver, P = make_solver()
+    u, _ = solver.compute(T(I0), T(I1))
+    u64, _ = oracle.tvl1_compute(I0, I1, P, dtype=np.float64)
+    e = epe(u.cpu().numpy(), u64)
+    assert e.mean() <= EPE_TOL, e.mean()
+
+
+def test_fused_matches_plain_form(cuda, pair24):
+    I0, I1, _ = pair24
+    solver, P = make_solver(max_warps=4, max_outer_iterations=60)
+    u, p = solver.compute(T(I0), T(I1))
+    z = torch.zeros((24, 24, 24, 3), device="cuda")
+    zp = torch.zeros((24, 24, 24, 3, 3), device="cuda")
+    u2, p2 = solver.compute_unfused(T(I0), T(I1), z, zp)
+    e = epe(u.cpu().numpy(), u2.cpu().numpy())
+    assert e.mean() < 1e-3 and e.max() < 2e-2, (e.mean(), e.max())
+
+
+@pytest.mark.parametrize("params", [dict(use_anisotropic_diff=False), dict(primaldual_algorithm_type=1),
+                                    dict(boundary_type="NEAREST"), dict(interpolation_type="LINEAR"),
+                                    dict(use_gaussian_blur=False, weight_tv=0.0), dict(num_scales=2),
+                                    dict(length_type="fixed", length=(1.0, 1.0, 1.0))])
+def test_fused_matches_oracle_other_options(cuda, oracle, params):
+    I0, I1, _ = synthetic.frame_pair((16, 18, 20), seed=11)
+    solver, P = make_solver(max_warps=3, max_outer_iterations=40, **params)
+    u, _ = solver.compute(T(I0), T(I1))
+    uo, _ = oracle.tvl1_compute(I0, I1, P, dtype=np.float32)
+    e = epe(u.cpu().numpy(), uo)
+    assert e.mean() < 5e-3 and e.max() < 0.1, (params, e.mean(), e.max())
+
+
+def test_warm_start_single_scale(cuda, oracle):
+    I0, I1, ut = synthetic.frame_pair((12, 13, 14), seed=5)
+    solver, P = make_solver(num_scales=1, max_warps=2, max_outer_iterations=30)
+    u0 = (ut * 0.5).astype(np.float32)
+    p0 = np.full((12, 13, 14, 3, 3), 0.01, np.float32)
+    u, p = solver.compute(T(I0), T(I1), T(u0), T(p0))
+    uo, _ = oracle.tvl1_compute(I0, I1, P, u=u0, p=p0, dtype=np.float32)
+    assert epe(u.cpu().numpy(), uo).mean() < 5e-3
+
+
+def test_batch_invariance_and_uneven_sizes(cuda):
+    """Each pair's result is bitwise the same alone and inside a batch of mixed sizes."""
+    shapes = [(24, 24, 24), (16, 24, 32), (40, 24, 16)]
+    pairs = [synthetic.frame_pair(s, seed=20 + i) for i, s in enumerate(shapes)]
+    solver, _ = make_solver(max_warps=3, max_outer_iterations=50)
+    together = solver.compute_batch([T(p[0]) for p in pairs], [T(p[1]) for p in pairs])
+    for (I0, I1, _), ub in zip(pairs, together):
+        ua = solver.compute_batch([T(I0)], [T(I1)])[0]
+        assert torch.equal(ua, ub)
+
+
+def test_tile_shapes_give_identical_results(cuda, pair24):
+    from singleventriclesegmentation_b200 import _lib
+    I0, I1, _ = pair24
+    solver, _ = make_solver(max_warps=2, max_outer_iterations=30)
+    ref = None
+    for tid in range(1, _lib.lib().svs_tvl1_num_tiles() + 1):
+        solver.tile_id = tid
+        solver._plans.clear()
+        u = solver.compute_batch([T(I0)], [T(I1)])[0]
+        if ref is None:
+            ref = u
+        assert torch.equal(u, ref), tid
+
+
+def test_graph_reuse_and_new_inputs(cuda):
+    solver, _ = make_solver(max_warps=2, max_outer_iterations=20)
+    a = synthetic.frame_pair((16, 16, 16), seed=1)
+    b = synthetic.frame_pair((16, 16, 16), seed=2)
+    ua1 = solver.compute_batch([T(a[0])], [T(a[1])])[0]
+    ub = solver.compute_batch([T(b[0])], [T(b[1])])[0]
+    ua2 = solver.compute_batch([T(a[0])], [T(a[1])])[0]
+    assert torch.equal(ua1, ua2) and not torch.equal(ua1, ub)
+
+
+@pytest.mark.parametrize("storage,tol", [("bf16", EPE_TOL), ("f16", EPE_TOL)])
+def test_reduced_storage_against_fp64_oracle(cuda, oracle, pair24, storage, tol):
+    I0, I1, _ = pair24
+    solver, P = make_solver(storage=storage)
+    u, _ = solver.compute(T(I0), T(I1))
+    u64, _ = oracle.tvl1_compute(I0, I1, P, dtype=np.float64)
+    e = epe(u.cpu().numpy(), u64)
+    print(f"{storage}: mean EPE {e.mean():.4g}, max {e.max():.4g}")
+    assert e.mean() <= tol
+
+
+def test_in_solve_median_equals_post_filter(cuda, pair24):
+    from singleventriclesegmentation_b200.flow_utils import apply_median_filter
+    I0, I1, _ = pair24
+    s1, _ = make_solver(max_warps=2, max_outer_iterations=20)
+    s2, _ = make_solver(max_warps=2, max_outer_iterations=20)
+    s2.median_kernel = 3
+    u = s1.compute_batch([T(I0)], [T(I1)])[0]
+    um = s2.compute_batch([T(I0)], [T(I1)])[0]
+    assert torch.equal(apply_median_filter(u, 3), um)
