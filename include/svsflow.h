@@ -176,8 +176,9 @@ svs_status svs_tvl1_plan_create(const svs_tvl1_params* params, int num_pairs,
 svs_status svs_tvl1_plan_destroy(svs_plan* plan);
 /* Bytes of device memory the plan holds. */
 size_t svs_tvl1_plan_device_bytes(const svs_plan* plan);
-/* Select the iteration tile (0 = automatic) for later solves; returns SVS_ERR_INVALID_ARG for
- * an unknown id. Used by the autotuner. */
+/* Select the iterate-kernel variant (0 = automatic) for later solves; SVS_ERR_INVALID_ARG for an
+ * unknown id. Variants 1-5 are TMA pipelines (32x8/5 stages, 32x8/4, 64x4/4, 16x16/4, 32x16/4),
+ * 6-8 plain-load forms (32x8, 32x4, 16x16). Used by the autotuner. */
 svs_status svs_tvl1_plan_set_tile(svs_plan* plan, int tile_id);
 int svs_tvl1_num_tiles(void);
 
@@ -192,6 +193,12 @@ svs_status svs_tvl1_solve_batch(svs_plan* plan, const svs_pair_desc* pairs_host,
 svs_status svs_tvl1_bench_iterations(svs_plan* plan, int level, int count, svs_stream_t stream);
 /* Number of kernel nodes in the plan's captured solve graph (0 before the first solve). */
 uint64_t svs_tvl1_plan_graph_kernels(const svs_plan* plan);
+/* Iterate-kernel variant the plan uses at a pyramid level (after the first solve; 0 before). */
+int svs_tvl1_plan_level_tile(const svs_plan* plan, int level);
+/* Synchronous check of the plan's device status: SVS_ERR_TIMEOUT if a bounded pipeline wait
+ * inside an iterate kernel gave up (the kernel then returned early and the results of that
+ * solve are invalid), SVS_OK otherwise. */
+svs_status svs_tvl1_plan_check(svs_plan* plan);
 
 /* Kernel-launch counter (all kernels this library launched in this process), for benchmarks. */
 uint64_t svs_launch_count(void);

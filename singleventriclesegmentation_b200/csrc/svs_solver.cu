@@ -18,8 +18,8 @@
 // dependency between the two half steps) and the new flow on the plane below. The only
 // per-iteration HBM traffic is read u, p, D, rc, gw and write u, p: 34 values per voxel.
 // The whole batched solve is captured once into a CUDA graph.
-#include <cuda_bf16.h>
-#include <cuda_fp16.h>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -29,61 +29,17 @@
 #include <vector>
 
 #include "svs_common.cuh"
+#include "svs_iterate.cuh"
 
 namespace svs {
 namespace {
 
-// ------------------------------------------------------------------------- storage conversions
-template <typename S> struct Store;
-template <> struct Store<float> {
-  static __device__ __forceinline__ float ld(const float* p) { return __ldg(p); }
-  static __device__ __forceinline__ float ld_plain(const float* p) { return *p; }
-  static __device__ __forceinline__ void st(float* p, float v) { *p = v; }
-};
-template <> struct Store<__nv_bfloat16> {
-  static __device__ __forceinline__ float ld(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
-  static __device__ __forceinline__ float ld_plain(const __nv_bfloat16* p) { return __bfloat162float(*p); }
-  static __device__ __forceinline__ void st(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
-};
-template <> struct Store<__half> {
-  static __device__ __forceinline__ float ld(const __half* p) { return __half2float(__ldg(p)); }
-  static __device__ __forceinline__ float ld_plain(const __half* p) { return __half2float(*p); }
-  static __device__ __forceinline__ void st(__half* p, float v) { *p = __float2half_rn(v); }
-};
-
-// One (pair, level) of the batch.
-struct Desc {
-  int nz, ny, nx, pad0;
-  float hz, hy, hx, pad1;
-  float lz, ly, lx, pad2;
-  long long n;
-  const float* I0;
-  const float* I1;
-  float* g1;
-  void* D;
-  void* rc;
-  void* gw;
-  void* u[2];
-  void* p[2];
-};
-
-// One CTA of the iterate kernel: a column tile [x0, x0+TX) x [y0, y0+TY) x [z0, z1).
-struct Tile {
-  int desc;
-  int x0, y0;
-  int z0z1;  // z0 | z1 << 16
-};
-
-struct IterArgs {
-  float sigma, tau, factor, wtv;
-  int src, bdry;
-};
-
+// Iterate-kernel variants compiled into the library (id 1..N; 0 = automatic).
 struct TileShape {
-  int tx, ty;
+  int tx, ty, nstg;  // nstg = 0: plain-load form; > 0: TMA form with that many stages
 };
-// The iterate-kernel tile shapes compiled into the library (id 1..N; 0 = automatic).
-constexpr TileShape kTileShapes[] = {{32, 8}, {32, 4}, {16, 8}, {64, 4}, {16, 16}, {32, 16}};
+constexpr TileShape kTileShapes[] = {{32, 8, 5}, {32, 8, 4}, {64, 4, 4}, {16, 16, 4}, {32, 16, 4},
+                                     {32, 8, 0}, {32, 4, 0}, {16, 16, 0}};
 constexpr int kNumTileShapes = sizeof(kTileShapes) / sizeof(kTileShapes[0]);
 
 // ------------------------------------------------------------------------------ small kernels
@@ -147,8 +103,9 @@ __global__ void restrict_kernel(const Desc* __restrict__ fine, const Desc* __res
 }
 
 // Per-level preparation, tvl13d.py:179-192: g1 = grad I1 (differentialOps.cu:540-655), the
-// anisotropic tensor from s, n, t1 (anisotropicDifferentialOps.cu:89-141) packed as a symmetric
-// matrix, and (coarsest level only) zero u and p.
+// anisotropic tensor from s, n, t1 (anisotropicDifferentialOps.cu:89-141) packed as the
+// symmetric matrix s n n^T + t1 t1^T (d00 d01 d02 d11 d12 d22), and (first level only) zero u, p.
+// Without anisotropy D is the identity (tvl13d.py:218-219, 231-232 skip the operator).
 template <typename S>
 __global__ void prepare_kernel(const Desc* __restrict__ descs, int use_aniso, float alpha,
                                float beta, int bdry, int zero_state, int src) {
@@ -184,14 +141,15 @@ __global__ void prepare_kernel(const Desc* __restrict__ descs, int use_aniso, fl
       for (int i = 0; i < 6; ++i) D[i] = 0.f;
     }
   }
+  const long long o = pidx(d, z, y, x);
   S* Dp = reinterpret_cast<S*>(d.D);
 #pragma unroll
-  for (int i = 0; i < 6; ++i) Store<S>::st(Dp + i * d.n + v, D[i]);
+  for (int i = 0; i < 6; ++i) Store<S>::st(Dp + i * d.cs + o, D[i]);
   if (zero_state) {
     S* u = reinterpret_cast<S*>(d.u[src]);
     S* p = reinterpret_cast<S*>(d.p[src]);
-    for (int i = 0; i < 3; ++i) Store<S>::st(u + i * d.n + v, 0.f);
-    for (int i = 0; i < 9; ++i) Store<S>::st(p + i * d.n + v, 0.f);
+    for (int i = 0; i < 3; ++i) Store<S>::st(u + i * d.cs + o, 0.f);
+    for (int i = 0; i < 9; ++i) Store<S>::st(p + i * d.cs + o, 0.f);
   }
 }
 
@@ -242,8 +200,9 @@ __global__ void linearise_kernel(const Desc* __restrict__ descs, int src, int in
   const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (v >= d.n) return;
   const int x = (int)(v % d.nx), y = (int)((v / d.nx) % d.ny), z = (int)(v / ((int64_t)d.nx * d.ny));
+  const long long o = pidx(d, z, y, x);
   const S* u = reinterpret_cast<const S*>(d.u[src]);
-  const float u0 = Store<S>::ld(u + v), u1 = Store<S>::ld(u + d.n + v), u2 = Store<S>::ld(u + 2 * d.n + v);
+  const float u0 = Store<S>::ld(u + o), u1 = Store<S>::ld(u + d.cs + o), u2 = Store<S>::ld(u + 2 * d.cs + o);
   const float cx = (float)x * d.hx + u0;
   const float cy = (float)y * d.hy + u1;
   const float cz = (float)z * d.hz + u2;
@@ -259,10 +218,10 @@ __global__ void linearise_kernel(const Desc* __restrict__ descs, int src, int in
   const float dot = u0 * s[1] + u1 * s[2] + u2 * s[3];
   const float rc = s[0] - dot - d.I0[v];
   S* gw = reinterpret_cast<S*>(d.gw);
-  Store<S>::st(reinterpret_cast<S*>(d.rc) + v, rc);
-  Store<S>::st(gw + v, s[1]);
-  Store<S>::st(gw + d.n + v, s[2]);
-  Store<S>::st(gw + 2 * d.n + v, s[3]);
+  Store<S>::st(reinterpret_cast<S*>(d.rc) + o, rc);
+  Store<S>::st(gw + o, s[1]);
+  Store<S>::st(gw + d.cs + o, s[2]);
+  Store<S>::st(gw + 2 * d.cs + o, s[3]);
 }
 
 // Coarse -> fine transfer of u (scaled by L_f/L_c per axis, tvl13d.py:151-153) and p
@@ -285,13 +244,15 @@ __global__ void prolong_kernel(const Desc* __restrict__ coarse, const Desc* __re
   const S* pc = reinterpret_cast<const S*>(c.p[src]);
   S* uf = reinterpret_cast<S*>(f.u[0]);
   S* pf = reinterpret_cast<S*>(f.p[0]);
+  const long long of = pidx(f, z, y, x);
   int ix, iy, iz;
   float wx, wy, wz;
   split_coord(cx, c.hx, ix, wx);
   split_coord(cy, c.hy, iy, wy);
   split_coord(cz, c.hz, iz, wz);
   for (int comp = 0; comp < 12; ++comp) {
-    const S* F = comp < 3 ? uc + comp * c.n : pc + (comp - 3) * c.n;
+    const S* F = comp < 3 ? uc + comp * c.cs : pc + (comp - 3) * c.cs;
+    auto at = [&](int zz, int yy, int xx) { return Store<S>::ld(F + pidx(c, zz, yy, xx)); };
     float val;
     if (interp == SVS_INTERPOLATE_CUBIC_HERMITESPLINE) {
       float bz[4];
@@ -300,9 +261,8 @@ __global__ void prolong_kernel(const Desc* __restrict__ coarse, const Desc* __re
         float by[4];
         for (int dy = 0; dy < 4; ++dy) {
           const int yy = fold(iy + dy - 1, c.ny, bdry);
-          const S* row = F + ((int64_t)zz * c.ny + yy) * c.nx;
-          by[dy] = hermite4(Store<S>::ld(row + fold(ix - 1, c.nx, bdry)), Store<S>::ld(row + fold(ix, c.nx, bdry)),
-                            Store<S>::ld(row + fold(ix + 1, c.nx, bdry)), Store<S>::ld(row + fold(ix + 2, c.nx, bdry)), wx);
+          by[dy] = hermite4(at(zz, yy, fold(ix - 1, c.nx, bdry)), at(zz, yy, fold(ix, c.nx, bdry)),
+                            at(zz, yy, fold(ix + 1, c.nx, bdry)), at(zz, yy, fold(ix + 2, c.nx, bdry)), wx);
         }
         bz[dz] = hermite4(by[0], by[1], by[2], by[3], wy);
       }
@@ -311,7 +271,6 @@ __global__ void prolong_kernel(const Desc* __restrict__ coarse, const Desc* __re
       const int x0 = fold(ix, c.nx, bdry), x1 = fold(ix + 1, c.nx, bdry);
       const int y0 = fold(iy, c.ny, bdry), y1 = fold(iy + 1, c.ny, bdry);
       const int z0 = fold(iz, c.nz, bdry), z1 = fold(iz + 1, c.nz, bdry);
-      auto at = [&](int zz, int yy, int xx) { return Store<S>::ld(F + ((int64_t)zz * c.ny + yy) * c.nx + xx); };
       val = (1 - wz) * (1 - wy) * (1 - wx) * at(z0, y0, x0);
       val += wz * (1 - wy) * (1 - wx) * at(z1, y0, x0);
       val += (1 - wz) * (1 - wy) * wx * at(z0, y0, x1);
@@ -321,15 +280,14 @@ __global__ void prolong_kernel(const Desc* __restrict__ coarse, const Desc* __re
       val += (1 - wz) * wy * wx * at(z0, y1, x1);
       val += wz * wy * wx * at(z1, y1, x1);
     } else {
-      const int xx = nearest_axis(cx, c.hx, c.nx, bdry), yy = nearest_axis(cy, c.hy, c.ny, bdry),
-                zz = nearest_axis(cz, c.hz, c.nz, bdry);
-      val = Store<S>::ld(F + ((int64_t)zz * c.ny + yy) * c.nx + xx);
+      val = at(nearest_axis(cz, c.hz, c.nz, bdry), nearest_axis(cy, c.hy, c.ny, bdry),
+               nearest_axis(cx, c.hx, c.nx, bdry));
     }
     if (comp < 3) {
       const float k = comp == 0 ? kx : (comp == 1 ? ky : kz);
-      Store<S>::st(uf + comp * f.n + v, val * k);
+      Store<S>::st(uf + comp * f.cs + of, val * k);
     } else {
-      Store<S>::st(pf + (comp - 3) * f.n + v, val);
+      Store<S>::st(pf + (comp - 3) * f.cs + of, val);
     }
   }
 }
@@ -341,13 +299,15 @@ __global__ void finalize_kernel(const Desc* __restrict__ descs, int src, float* 
   const Desc d = descs[blockIdx.y];
   const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (v >= d.n) return;
+  const int x = (int)(v % d.nx), y = (int)((v / d.nx) % d.ny), z = (int)(v / ((int64_t)d.nx * d.ny));
+  const long long o = pidx(d, z, y, x);
   const S* u = reinterpret_cast<const S*>(d.u[src]);
   float* uo = u_out[blockIdx.y];
-  for (int c = 0; c < 3; ++c) uo[3 * v + c] = Store<S>::ld(u + c * d.n + v);
+  for (int c = 0; c < 3; ++c) uo[3 * v + c] = Store<S>::ld(u + c * d.cs + o);
   float* po = p_out[blockIdx.y];
   if (po) {
     const S* p = reinterpret_cast<const S*>(d.p[src]);
-    for (int c = 0; c < 9; ++c) po[9 * v + c] = Store<S>::ld(p + c * d.n + v);
+    for (int c = 0; c < 9; ++c) po[9 * v + c] = Store<S>::ld(p + c * d.cs + o);
   }
 }
 
@@ -359,239 +319,21 @@ __global__ void warm_start_kernel(const Desc* __restrict__ descs, const float* c
   const Desc d = descs[blockIdx.y];
   const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (v >= d.n) return;
+  const int x = (int)(v % d.nx), y = (int)((v / d.nx) % d.ny), z = (int)(v / ((int64_t)d.nx * d.ny));
+  const long long o = pidx(d, z, y, x);
   const float* ui = u_in[blockIdx.y];
   const float* pi = p_in[blockIdx.y];
   S* u = reinterpret_cast<S*>(d.u[0]);
   S* p = reinterpret_cast<S*>(d.p[0]);
-  for (int c = 0; c < 3; ++c) Store<S>::st(u + c * d.n + v, ui ? ui[3 * v + c] : 0.f);
-  for (int c = 0; c < 9; ++c) Store<S>::st(p + c * d.n + v, pi ? pi[9 * v + c] : 0.f);
-}
-
-// ----------------------------------------------------------------------------- iterate kernel
-// One primal-dual iteration (tvl13d.py:213-253) over a column tile, marching along z.
-//
-// Thread (tx, ty) of the (TX+2) x (TY+2) block owns column (x0-1+tx, y0-1+ty) of the "dual
-// region" (tile plus a one-voxel halo). At plane k the block
-//   1. publishes u(k) of its columns (and a second halo ring) to shared memory,
-//   2. computes on the dual region (minus its 4 corners) p_new(k) = proj(p + sigma D grad u)
-//      and q = D p_new, keeping the z-row of q in registers and publishing the x- and y-rows,
-//   3. on the tile interior, finishes plane k-1: div = adjoint(q) from the published rows and
-//      the registers of planes k-2 and k, then u_new(k-1) = prox_primal(u - tau div).
-// One __syncthreads per plane. Halo duals are recomputed by neighbouring tiles, so each
-// launch is independent of every other tile of the same launch (ping-pong u and p).
-template <typename S, int TX, int TY>
-__global__ void __launch_bounds__((TX + 2) * (TY + 2))
-iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, IterArgs a) {
-  constexpr int PX = TX + 2, PY = TY + 2, UX = TX + 4, UY = TY + 4;
-  constexpr int NRING = 2 * (TX + TY);
-  __shared__ float su[2][3][UY][UX];
-  __shared__ float sq[2][6][PY][PX];
-
-  const Tile T = tiles[blockIdx.x];
-  const Desc& Dg = descs[T.desc];
-  const int nz = Dg.nz, ny = Dg.ny, nx = Dg.nx;
-  const float hz = Dg.hz, hy = Dg.hy, hx = Dg.hx;
-  const int64_t n = Dg.n;
-  const int z0 = T.z0z1 & 0xffff, z1 = T.z0z1 >> 16;
-  const S* __restrict__ u_src = reinterpret_cast<const S*>(Dg.u[a.src]);
-  const S* __restrict__ p_src = reinterpret_cast<const S*>(Dg.p[a.src]);
-  S* __restrict__ u_dst = reinterpret_cast<S*>(Dg.u[a.src ^ 1]);
-  S* __restrict__ p_dst = reinterpret_cast<S*>(Dg.p[a.src ^ 1]);
-  const S* __restrict__ Dm = reinterpret_cast<const S*>(Dg.D);
-  const S* __restrict__ rcm = reinterpret_cast<const S*>(Dg.rc);
-  const S* __restrict__ gwm = reinterpret_cast<const S*>(Dg.gw);
-
-  const int tid = threadIdx.x;
-  const int tx = tid % PX, ty = tid / PX;
-  const int gx = T.x0 - 1 + tx, gy = T.y0 - 1 + ty;
-  const bool in_dom = gx >= 0 && gx < nx && gy >= 0 && gy < ny;
-  const bool corner = (tx == 0 || tx == PX - 1) && (ty == 0 || ty == PY - 1);
-  const bool dual_on = in_dom && !corner;
-  const bool interior = in_dom && tx >= 1 && tx <= TX && ty >= 1 && ty <= TY;
-  const int64_t col = (int64_t)gy * nx + gx;  // voxel index of this column at z = 0
-  const int64_t plane = (int64_t)nx * ny;
-
-  // second halo ring (u only): cells at distance 2 from the tile along x or y
-  int rx = -1, ry = -1;
-  if (tid < NRING) {
-    int r = tid;
-    if (r < TY) { rx = 0; ry = 2 + r; }
-    else if ((r -= TY) < TY) { rx = UX - 1; ry = 2 + r; }
-    else if ((r -= TY) < TX) { rx = 2 + r; ry = 0; }
-    else { r -= TX; rx = 2 + r; ry = UY - 1; }
-  }
-  const int rgx = T.x0 - 2 + rx, rgy = T.y0 - 2 + ry;
-  const bool ring_on = tid < NRING && rgx >= 0 && rgx < nx && rgy >= 0 && rgy < ny;
-  const int64_t rcol = (int64_t)rgy * nx + rgx;
-
-  const int kb = max(z0 - 1, 0), ke = min(z1, nz - 1);
-  float um[3] = {0.f, 0.f, 0.f}, uc[3] = {0.f, 0.f, 0.f}, up[3] = {0.f, 0.f, 0.f};
-  if (in_dom) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      if (kb >= 1) um[c] = Store<S>::ld(u_src + c * n + (kb - 1) * plane + col);
-      uc[c] = Store<S>::ld(u_src + c * n + kb * plane + col);
-      if (kb + 1 < nz) up[c] = Store<S>::ld(u_src + c * n + (kb + 1) * plane + col);
-    }
-  }
-  float qzmm[3] = {0.f, 0.f, 0.f}, qzm[3] = {0.f, 0.f, 0.f}, qzc[3] = {0.f, 0.f, 0.f};
-  const float sigma = a.sigma, tau = a.tau, factor = a.factor, wtv = a.wtv;
-  const int bdry = a.bdry;
-
-  for (int k = kb; k <= ke; ++k) {
-    const int slot = k & 1;
-    // --- loads for this step (issued before the barrier)
-    float pk[9], Dk[6];
-    if (dual_on) {
-      const int64_t o = k * plane + col;
-#pragma unroll
-      for (int c = 0; c < 9; ++c) pk[c] = Store<S>::ld(p_src + c * n + o);
-#pragma unroll
-      for (int c = 0; c < 6; ++c) Dk[c] = Store<S>::ld(Dm + c * n + o);
-    }
-    const int j = k - 1;  // plane finished in this step
-    const bool primal_on = interior && j >= z0 && j < z1;
-    float rcj = 0.f, gj[3] = {0.f, 0.f, 0.f};
-    if (primal_on) {
-      const int64_t o = j * plane + col;
-      rcj = Store<S>::ld(rcm + o);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) gj[c] = Store<S>::ld(gwm + c * n + o);
-    }
-    // --- 1. publish u(k)
-    if (in_dom) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) su[slot][c][ty + 1][tx + 1] = uc[c];
-    }
-    if (ring_on) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) su[slot][c][ry][rx] = Store<S>::ld(u_src + c * n + k * plane + rcol);
-    }
-    __syncthreads();
-    // --- 2. dual step at plane k
-    if (dual_on) {
-      float pn[9];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float ex = fwd_axis(su[slot][c][ty + 1][tx], uc[c], su[slot][c][ty + 1][tx + 2], gx, nx, bdry, hx);
-        const float ey = fwd_axis(su[slot][c][ty][tx + 1], uc[c], su[slot][c][ty + 2][tx + 1], gy, ny, bdry, hy);
-        const float ez = fwd_axis(um[c], uc[c], up[c], k, nz, bdry, hz);
-        const float dz0 = Dk[0] * ex + Dk[1] * ey + Dk[2] * ez;
-        const float dz1 = Dk[1] * ex + Dk[3] * ey + Dk[4] * ez;
-        const float dz2 = Dk[2] * ex + Dk[4] * ey + Dk[5] * ez;
-        const float v0 = pk[3 * c] + sigma * dz0;
-        const float v1 = pk[3 * c + 1] + sigma * dz1;
-        const float v2 = pk[3 * c + 2] + sigma * dz2;
-        // projection onto the ball of radius weight_tv, opticalFlowOps.cu:193-206
-        const float den = fmaxf(1.0f, sqrtf(v0 * v0 + v1 * v1 + v2 * v2) / wtv);
-        if (wtv > 0.f) {
-          pn[3 * c] = v0 / den;
-          pn[3 * c + 1] = v1 / den;
-          pn[3 * c + 2] = v2 / den;
-        } else {  // tvl13d.py:223-224
-          pn[3 * c] = pn[3 * c + 1] = pn[3 * c + 2] = 0.f;
-        }
-      }
-      if (interior && k >= z0 && k < z1) {
-        const int64_t o = k * plane + col;
-#pragma unroll
-        for (int c = 0; c < 9; ++c) Store<S>::st(p_dst + c * n + o, pn[c]);
-      }
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float q0 = Dk[0] * pn[3 * c] + Dk[1] * pn[3 * c + 1] + Dk[2] * pn[3 * c + 2];
-        const float q1 = Dk[1] * pn[3 * c] + Dk[3] * pn[3 * c + 1] + Dk[4] * pn[3 * c + 2];
-        const float q2 = Dk[2] * pn[3 * c] + Dk[4] * pn[3 * c + 1] + Dk[5] * pn[3 * c + 2];
-        sq[slot][c][ty][tx] = q0;
-        sq[slot][3 + c][ty][tx] = q1;
-        qzc[c] = q2;
-      }
-    }
-    // --- 3. primal step at plane j = k-1 (its x/y rows were published in the previous step)
-    if (primal_on) {
-      const int ps = slot ^ 1;
-      float un[3];
-      const float rho = rcj + (um[0] * gj[0] + um[1] * gj[1] + um[2] * gj[2]);
-      const float g2s = gj[0] * gj[0] + gj[1] * gj[1] + gj[2] * gj[2];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float ax = adj_axis(sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1], gx, nx, bdry);
-        const float ay = adj_axis(sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx], gy, ny, bdry);
-        const float az = adj_axis(qzmm[c], qzm[c], qzc[c], j, nz, bdry);
-        const float div = (ax / hx + ay / hy) + az / hz;
-        un[c] = um[c] - tau * div;
-      }
-      // L1 data-term shrinkage, opticalFlowOps.cu:140-171
-      if (rho < -factor * g2s) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) un[c] += factor * gj[c];
-      } else if (rho > factor * g2s) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) un[c] += -factor * gj[c];
-      } else if (g2s > 1e-10f) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) un[c] += -rho * gj[c] / g2s;
-      }
-      const int64_t o = j * plane + col;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) Store<S>::st(u_dst + c * n + o, un[c]);
-    }
-    // --- roll the z window
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      qzmm[c] = qzm[c];
-      qzm[c] = qzc[c];
-      um[c] = uc[c];
-      uc[c] = up[c];
-      up[c] = 0.f;
-    }
-    if (in_dom && k + 2 < nz) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) up[c] = Store<S>::ld(u_src + c * n + (k + 2) * plane + col);
-    }
-  }
-  // last plane of the volume: its dual rows were published in the final step
-  if (z1 >= nz) {
-    __syncthreads();
-    const int j = nz - 1;
-    if (interior && j >= z0) {
-      const int ps = j & 1;
-      const int64_t o = j * plane + col;
-      const float rcj = Store<S>::ld(rcm + o);
-      float gj[3], un[3];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) gj[c] = Store<S>::ld(gwm + c * n + o);
-      const float rho = rcj + (um[0] * gj[0] + um[1] * gj[1] + um[2] * gj[2]);
-      const float g2s = gj[0] * gj[0] + gj[1] * gj[1] + gj[2] * gj[2];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float ax = adj_axis(sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1], gx, nx, bdry);
-        const float ay = adj_axis(sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx], gy, ny, bdry);
-        const float az = adj_axis(qzmm[c], qzm[c], 0.f, j, nz, bdry);
-        const float div = (ax / hx + ay / hy) + az / hz;
-        un[c] = um[c] - tau * div;
-      }
-      if (rho < -factor * g2s) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) un[c] += factor * gj[c];
-      } else if (rho > factor * g2s) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) un[c] += -factor * gj[c];
-      } else if (g2s > 1e-10f) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) un[c] += -rho * gj[c] / g2s;
-      }
-#pragma unroll
-      for (int c = 0; c < 3; ++c) Store<S>::st(u_dst + c * n + o, un[c]);
-    }
-  }
+  for (int c = 0; c < 3; ++c) Store<S>::st(u + c * d.cs + o, ui ? ui[3 * v + c] : 0.f);
+  for (int c = 0; c < 9; ++c) Store<S>::st(p + c * d.cs + o, pi ? pi[9 * v + c] : 0.f);
 }
 
 }  // namespace
 }  // namespace svs
 
 // =============================================================================================
-// Host side: plan (device state + tile lists), the enqueue sequence, CUDA-graph capture.
+// Host side: plan (device state, tile lists, TMA descriptors), the enqueue sequence, CUDA graph.
 // =============================================================================================
 struct svs_plan {
   svs_tvl1_params prm{};
@@ -600,12 +342,15 @@ struct svs_plan {
   std::vector<int> dims;                   // level-0 dims, 3 per pair
   std::vector<svs::Desc> h_descs;          // [levels][pairs]
   svs::Desc* d_descs = nullptr;
+  svs::TMaps* d_maps = nullptr;            // [levels][pairs], for the tile shape in use
   std::vector<std::vector<svs::Tile>> h_tiles;  // per level
   std::vector<svs::Tile*> d_tiles;
-  int tile_id = 0;                         // 0 = automatic
+  std::vector<int> level_tile;             // tile id used per level
+  int tile_id = 0;                         // requested (0 = automatic)
   int tiles_built_for = -1;
   void* arena = nullptr;
   size_t arena_bytes = 0;
+  int* d_status = nullptr;                 // device error bits (SVS_DEV_*)
   float** d_raw = nullptr;                 // [2*pairs] raw input frames (device)
   float** d_uout = nullptr;                // [pairs] AoS u results
   float** d_pout = nullptr;                // [pairs] AoS p results (or null entries)
@@ -632,69 +377,164 @@ namespace {
 
 size_t storage_bytes(int storage) { return storage == SVS_STORAGE_F32 ? 4 : 2; }
 
-// Automatic tile choice for a level: 32x8 columns; z is split into chunks only when the batch
-// has too few column tiles to fill the GPU (single small pairs).
-int auto_tile(const svs_plan& P, int level) {
-  (void)P;
-  (void)level;
-  return 1;
+// ---------------------------------------------------------------------- TMA tensor maps
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
 }
 
-void build_tiles(svs_plan& P, int tile_id) {
-  P.h_tiles.assign(P.levels, {});
-  for (int l = 0; l < P.levels; ++l) {
-    const int tid = tile_id > 0 ? tile_id : auto_tile(P, l);
-    const TileShape ts = kTileShapes[tid - 1];
-    long long xy_tiles = 0;
-    for (int i = 0; i < P.num_pairs; ++i) {
-      const Desc& d = P.h_descs[(size_t)l * P.num_pairs + i];
-      xy_tiles += (long long)ceil_div(d.nx, ts.tx) * ceil_div(d.ny, ts.ty);
-    }
-    const long long target = 148LL * 4;
-    for (int i = 0; i < P.num_pairs; ++i) {
-      const Desc& d = P.h_descs[(size_t)l * P.num_pairs + i];
-      int chunks = 1;
-      if (xy_tiles < target) chunks = (int)std::min<long long>((target + xy_tiles - 1) / xy_tiles, std::max(1, d.nz / 8));
-      const int zc = (d.nz + chunks - 1) / chunks;
-      for (int z0 = 0; z0 < d.nz; z0 += zc)
-        for (int y0 = 0; y0 < d.ny; y0 += ts.ty)
-          for (int x0 = 0; x0 < d.nx; x0 += ts.tx) {
-            const int z1 = std::min(d.nz, z0 + zc);
-            P.h_tiles[l].push_back(Tile{l * P.num_pairs + i, x0, y0, z0 | (z1 << 16)});
-          }
-    }
+// A 4D map (x, y, z, component) over one pitched planar field, box {bx, by, 1, bc}.
+bool encode_field(CUtensorMap* m, int storage, const void* base, const Desc& d, int comps, int bx, int by) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  const CUtensorMapDataType dt = storage == SVS_STORAGE_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                 : storage == SVS_STORAGE_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                               : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+  const cuuint64_t es = storage_bytes(storage);
+  cuuint64_t gdim[4] = {(cuuint64_t)d.nx, (cuuint64_t)d.ny, (cuuint64_t)d.nz, (cuuint64_t)comps};
+  cuuint64_t gstride[3] = {(cuuint64_t)d.pitch * es, (cuuint64_t)d.pitch * d.ny * es, (cuuint64_t)d.cs * es};
+  cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1u, (cuuint32_t)comps};
+  cuuint32_t estride[4] = {1, 1, 1, 1};
+  const CUresult r = fn(m, dt, 4, const_cast<void*>(base), gdim, gstride, box, estride,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <typename S, int TX, int TY, int NSTG>
+bool encode_maps(svs_plan& P, std::vector<TMaps>& maps, int level) {
+  using G = TmaGeom<S, TX, TY, NSTG>;
+  for (int i = 0; i < P.num_pairs; ++i) {
+    const size_t k = (size_t)level * P.num_pairs + i;
+    const Desc& d = P.h_descs[k];
+    TMaps& m = maps[k];
+    const int st = P.prm.storage;
+    bool ok = encode_field(&m.u[0], st, d.u[0], d, 3, G::UXB, G::UYB) &&
+              encode_field(&m.u[1], st, d.u[1], d, 3, G::UXB, G::UYB) &&
+              encode_field(&m.p[0], st, d.p[0], d, 9, G::PXB, G::PYB) &&
+              encode_field(&m.p[1], st, d.p[1], d, 9, G::PXB, G::PYB) &&
+              encode_field(&m.D, st, d.D, d, 6, G::PXB, G::PYB) &&
+              encode_field(&m.rc, st, d.rc, d, 1, TX, TY) && encode_field(&m.gw, st, d.gw, d, 3, TX, TY);
+    if (!ok) return false;
+  }
+  return true;
+}
+
+template <typename S, int TX, int TY, int NSTG>
+bool tma_prepare(svs_plan& P, std::vector<TMaps>& maps, int level) {
+  using G = TmaGeom<S, TX, TY, NSTG>;
+  if (G::SMEM > 227 * 1024) return false;
+  if (cudaFuncSetAttribute(iterate_tma_kernel<S, TX, TY, NSTG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           G::SMEM) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return encode_maps<S, TX, TY, NSTG>(P, maps, level);
+}
+
+// Dispatch over the compiled variants. `op` 0: prepare (attributes + maps), 1: launch.
+template <typename S>
+bool iter_variant(svs_plan& P, std::vector<TMaps>* maps, int level, int tid, int op, const IterArgs* a,
+                  cudaStream_t s) {
+  const unsigned nt = (unsigned)P.h_tiles[level].size();
+  const Tile* tl = P.d_tiles.empty() ? nullptr : P.d_tiles[level];
+#define SVS_TMA_CASE(ID, TX, TY, NS)                                                                  \
+  case ID:                                                                                            \
+    if (op == 0) return tma_prepare<S, TX, TY, NS>(P, *maps, level);                                   \
+    iterate_tma_kernel<S, TX, TY, NS><<<nt, (TX + 2) * (TY + 2), TmaGeom<S, TX, TY, NS>::SMEM, s>>>(  \
+        tl, P.d_descs, P.d_maps, *a, P.d_status);                                                     \
+    return true;
+#define SVS_PLAIN_CASE(ID, TX, TY)                                                                   \
+  case ID:                                                                                           \
+    if (op == 0) return true;                                                                        \
+    iterate_kernel<S, TX, TY><<<nt, (TX + 2) * (TY + 2), 0, s>>>(tl, P.d_descs, *a);                 \
+    return true;
+  switch (tid) {
+    SVS_TMA_CASE(1, 32, 8, 5)
+    SVS_TMA_CASE(2, 32, 8, 4)
+    SVS_TMA_CASE(3, 64, 4, 4)
+    SVS_TMA_CASE(4, 16, 16, 4)
+    SVS_TMA_CASE(5, 32, 16, 4)
+    SVS_PLAIN_CASE(6, 32, 8)
+    SVS_PLAIN_CASE(7, 32, 4)
+    SVS_PLAIN_CASE(8, 16, 16)
+    default: return false;
+  }
+#undef SVS_TMA_CASE
+#undef SVS_PLAIN_CASE
+}
+
+bool iter_dispatch(svs_plan& P, std::vector<TMaps>* maps, int level, int tid, int op, const IterArgs* a,
+                   cudaStream_t s) {
+  if (P.prm.storage == SVS_STORAGE_BF16) return iter_variant<__nv_bfloat16>(P, maps, level, tid, op, a, s);
+  if (P.prm.storage == SVS_STORAGE_F16) return iter_variant<__half>(P, maps, level, tid, op, a, s);
+  return iter_variant<float>(P, maps, level, tid, op, a, s);
+}
+
+// Automatic choice: the 5-stage 32x8 TMA pipeline for 4-byte storage, the 4-stage one (two CTAs
+// per SM) for 2-byte storage; the plain-load 32x8 form if TMA descriptors cannot be built.
+int auto_tile(const svs_plan& P) { return P.prm.storage == SVS_STORAGE_F32 ? 1 : 2; }
+
+void build_tiles(svs_plan& P, int level, int tid) {
+  const TileShape ts = kTileShapes[tid - 1];
+  std::vector<Tile>& out = P.h_tiles[level];
+  out.clear();
+  long long xy_tiles = 0;
+  for (int i = 0; i < P.num_pairs; ++i) {
+    const Desc& d = P.h_descs[(size_t)level * P.num_pairs + i];
+    xy_tiles += (long long)ceil_div(d.nx, ts.tx) * ceil_div(d.ny, ts.ty);
+  }
+  // z is split into chunks only when the level has too few column tiles to fill the GPU
+  const long long target = 148LL * 2;
+  for (int i = 0; i < P.num_pairs; ++i) {
+    const Desc& d = P.h_descs[(size_t)level * P.num_pairs + i];
+    int chunks = 1;
+    if (xy_tiles < target)
+      chunks = (int)std::min<long long>((target + xy_tiles - 1) / xy_tiles, std::max(1, d.nz / 8));
+    const int zc = (d.nz + chunks - 1) / chunks;
+    for (int z0 = 0; z0 < d.nz; z0 += zc)
+      for (int y0 = 0; y0 < d.ny; y0 += ts.ty)
+        for (int x0 = 0; x0 < d.nx; x0 += ts.tx) {
+          const int z1 = std::min(d.nz, z0 + zc);
+          out.push_back(Tile{level * P.num_pairs + i, x0, y0, z0 | (z1 << 16)});
+        }
   }
 }
 
-svs_status upload_tiles(svs_plan& P) {
+// (Re)build tile lists and TMA descriptors for the requested tile id.
+svs_status setup_tiles(svs_plan& P) {
+  const int want = P.tile_id;
+  P.h_tiles.assign(P.levels, {});
+  P.level_tile.assign(P.levels, 0);
+  std::vector<TMaps> maps((size_t)P.levels * P.num_pairs);
+  std::memset(maps.data(), 0, maps.size() * sizeof(TMaps));
+  for (int l = 0; l < P.levels; ++l) {
+    int tid = want > 0 ? want : auto_tile(P);
+    build_tiles(P, l, tid);
+    if (!iter_dispatch(P, &maps, l, tid, 0, nullptr, nullptr)) {
+      if (want > 0) return fail(SVS_ERR_UNSUPPORTED, "tile variant not usable for this plan (shared memory or TMA descriptor limits)");
+      tid = 6;  // plain-load 32x8
+      build_tiles(P, l, tid);
+    }
+    P.level_tile[l] = tid;
+  }
   for (auto* p : P.d_tiles) cudaFree(p);
   P.d_tiles.assign(P.levels, nullptr);
   for (int l = 0; l < P.levels; ++l) {
     const size_t bytes = P.h_tiles[l].size() * sizeof(Tile);
     svs_status st = check_cuda(cudaMalloc(&P.d_tiles[l], bytes), "tile list");
-    if (st) return st;
-    st = check_cuda(cudaMemcpy(P.d_tiles[l], P.h_tiles[l].data(), bytes, cudaMemcpyHostToDevice), "tile list");
+    if (!st) st = check_cuda(cudaMemcpy(P.d_tiles[l], P.h_tiles[l].data(), bytes, cudaMemcpyHostToDevice), "tile list");
     if (st) return st;
   }
-  return SVS_OK;
-}
-
-template <typename S, int TX, int TY>
-void launch_iter(const svs_plan& P, int level, const IterArgs& a, cudaStream_t s) {
-  const unsigned nt = (unsigned)P.h_tiles[level].size();
-  iterate_kernel<S, TX, TY><<<nt, (TX + 2) * (TY + 2), 0, s>>>(P.d_tiles[level], P.d_descs, a);
-}
-
-template <typename S>
-void launch_iter_shape(const svs_plan& P, int level, int tid, const IterArgs& a, cudaStream_t s) {
-  switch (tid) {
-    case 1: launch_iter<S, 32, 8>(P, level, a, s); break;
-    case 2: launch_iter<S, 32, 4>(P, level, a, s); break;
-    case 3: launch_iter<S, 16, 8>(P, level, a, s); break;
-    case 4: launch_iter<S, 64, 4>(P, level, a, s); break;
-    case 5: launch_iter<S, 16, 16>(P, level, a, s); break;
-    default: launch_iter<S, 32, 16>(P, level, a, s); break;
-  }
+  return check_cuda(cudaMemcpy(P.d_maps, maps.data(), maps.size() * sizeof(TMaps), cudaMemcpyHostToDevice), "tensor maps");
 }
 
 long long max_voxels(const svs_plan& P, int level) {
@@ -703,8 +543,19 @@ long long max_voxels(const svs_plan& P, int level) {
   return m;
 }
 
+IterArgs iter_args(const svs_plan& P, int it, int cur) {
+  IterArgs a;
+  a.sigma = P.sig_sched.empty() ? (float)P.prm.sigma : P.sig_sched[it];
+  a.tau = P.tau_sched.empty() ? (float)P.prm.tau : P.tau_sched[it];
+  a.factor = a.tau * P.prm.weight_matching;  // opticalFlowOps.cu:440
+  a.wtv = P.prm.weight_tv;
+  a.src = cur;
+  a.bdry = P.prm.boundary;
+  return a;
+}
+
 // The whole batched solve as a sequence of launches on stream s. Returns the number of kernel
-// launches issued (for the launch counter) or -1 after a launch error.
+// launches issued or -1 after a launch error.
 template <typename S>
 long long enqueue_solve(svs_plan& P, cudaStream_t s) {
   const svs_tvl1_params& q = P.prm;
@@ -723,24 +574,16 @@ long long enqueue_solve(svs_plan& P, cudaStream_t s) {
     ++launches;
   }
   int cur = 0;
-  const float wm = q.weight_matching;
   for (int l = L - 1; l >= 0; --l) {
     const int zero = (l == L - 1) && !(P.warm && L == 1);
     prepare_kernel<S><<<grid(l), 256, 0, s>>>(D + (size_t)l * np, q.use_anisotropic_diff, q.alpha, q.beta, q.boundary, zero, cur);
     ++launches;
-    const int tid = P.tile_id > 0 ? P.tile_id : auto_tile(P, l);
     for (int w = 0; w < q.max_warps; ++w) {
       linearise_kernel<S><<<grid(l), 256, 0, s>>>(D + (size_t)l * np, cur, q.interpolation, q.boundary);
       ++launches;
       for (int it = 0; it < q.max_outer_iterations; ++it) {
-        IterArgs a;
-        a.sigma = P.sig_sched[it];
-        a.tau = P.tau_sched[it];
-        a.factor = a.tau * wm;  // opticalFlowOps.cu:440
-        a.wtv = q.weight_tv;
-        a.src = cur;
-        a.bdry = q.boundary;
-        launch_iter_shape<S>(P, l, tid, a, s);
+        const IterArgs a = iter_args(P, it, cur);
+        iter_dispatch(P, nullptr, l, P.level_tile[l], 1, &a, s);
         ++launches;
         cur ^= 1;
       }
@@ -810,6 +653,7 @@ svs_status svs_tvl1_plan_create(const svs_tvl1_params* prm, int num_pairs, const
   P->h_descs.resize((size_t)P->levels * num_pairs);
   size_t bytes = 0;
   const size_t sb = storage_bytes(prm->storage);
+  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
   for (int i = 0; i < num_pairs; ++i) {
     int nz = dims[3 * i], ny = dims[3 * i + 1], nx = dims[3 * i + 2];
     if (nz >= 65535 || ny >= 65535 || nx >= 65535) { delete P; return fail(SVS_ERR_INVALID_ARG, "svs_tvl1_plan_create: volume dimension too large"); }
@@ -822,37 +666,43 @@ svs_status svs_tvl1_plan_create(const svs_tvl1_params* prm, int num_pairs, const
       Desc& d = P->h_descs[(size_t)l * num_pairs + i];
       std::memset(&d, 0, sizeof(d));
       d.nz = nz; d.ny = ny; d.nx = nx;
+      d.pitch = (nx + 7) / 8 * 8;
       d.n = (long long)nz * ny * nx;
+      d.cs = (long long)d.pitch * ny * nz;
       if (prm->length_type == 0) { d.lz = (float)(nz - 1); d.ly = (float)(ny - 1); d.lx = (float)(nx - 1); }
       else { d.lz = prm->length_z; d.ly = prm->length_y; d.lx = prm->length_x; }
       d.hz = d.lz / (float)(nz - 1); d.hy = d.ly / (float)(ny - 1); d.hx = d.lx / (float)(nx - 1);
-      const size_t n = (size_t)d.n;
-      bytes += 5 * ((n * 4 + 255) / 256 * 256);           // I0, I1, g1 (3 planes)
-      bytes += (6 + 1 + 3 + 6 + 18) * ((n * sb + 255) / 256 * 256) + 34 * 256;
-      if (l == 0) bytes += (2 + 3 + 3 + 9) * ((n * 4 + 255) / 256 * 256);  // raw x2, uout, umed, pout
+      const size_t n = (size_t)d.n, cs = (size_t)d.cs;
+      bytes += 2 * al(n * 4) + al(3 * n * 4);                       // I0, I1, g1
+      bytes += al(6 * cs * sb) + al(cs * sb) + al(3 * cs * sb);      // D, rc, gw
+      bytes += 2 * al(3 * cs * sb) + 2 * al(9 * cs * sb);            // u[2], p[2]
+      if (l == 0) bytes += 2 * al(n * 4) + 2 * al(3 * n * 4) + al(9 * n * 4);  // raw x2, uout, umed, pout
     }
   }
   bytes += 4096;
   svs_status st = check_cuda(cudaMalloc(&P->arena, bytes), "svs_tvl1_plan_create: device state");
   if (st) { delete P; return st; }
   P->arena_bytes = bytes;
+  // zero the whole arena once: pitch padding and planes never written stay zero
+  st = check_cuda(cudaMemset(P->arena, 0, bytes), "svs_tvl1_plan_create");
+  if (st) { svs_tvl1_plan_destroy(P); return st; }
   char* cur = reinterpret_cast<char*>(P->arena);
   P->raw.resize(2 * num_pairs); P->uout.resize(num_pairs); P->pout.resize(num_pairs); P->umed.resize(num_pairs);
   P->uinit.assign(num_pairs, nullptr); P->pinit.assign(num_pairs, nullptr);
   for (int l = 0; l < P->levels; ++l)
     for (int i = 0; i < num_pairs; ++i) {
       Desc& d = P->h_descs[(size_t)l * num_pairs + i];
-      const size_t n = (size_t)d.n;
+      const size_t n = (size_t)d.n, cs = (size_t)d.cs;
       d.I0 = carve<float>(cur, n);
       d.I1 = carve<float>(cur, n);
       d.g1 = carve<float>(cur, 3 * n);
-      d.D = carve<char>(cur, 6 * n * sb);
-      d.rc = carve<char>(cur, n * sb);
-      d.gw = carve<char>(cur, 3 * n * sb);
-      d.u[0] = carve<char>(cur, 3 * n * sb);
-      d.u[1] = carve<char>(cur, 3 * n * sb);
-      d.p[0] = carve<char>(cur, 9 * n * sb);
-      d.p[1] = carve<char>(cur, 9 * n * sb);
+      d.D = carve<char>(cur, 6 * cs * sb);
+      d.rc = carve<char>(cur, cs * sb);
+      d.gw = carve<char>(cur, 3 * cs * sb);
+      d.u[0] = carve<char>(cur, 3 * cs * sb);
+      d.u[1] = carve<char>(cur, 3 * cs * sb);
+      d.p[0] = carve<char>(cur, 9 * cs * sb);
+      d.p[1] = carve<char>(cur, 9 * cs * sb);
       if (l == 0) {
         P->raw[2 * i] = carve<float>(cur, n);
         P->raw[2 * i + 1] = carve<float>(cur, n);
@@ -874,6 +724,9 @@ svs_status svs_tvl1_plan_create(const svs_tvl1_params* prm, int num_pairs, const
   if (!st) st = upload((void**)&P->d_pout, nop.data(), nop.size() * sizeof(float*));
   if (!st) st = upload((void**)&P->d_uinit, P->uinit.data(), P->uinit.size() * sizeof(float*));
   if (!st) st = upload((void**)&P->d_pinit, P->pinit.data(), P->pinit.size() * sizeof(float*));
+  if (!st) st = check_cuda(cudaMalloc((void**)&P->d_maps, (size_t)P->levels * num_pairs * sizeof(TMaps)), "svs_tvl1_plan_create");
+  if (!st) st = check_cuda(cudaMalloc((void**)&P->d_status, sizeof(int)), "svs_tvl1_plan_create");
+  if (!st) st = check_cuda(cudaMemset(P->d_status, 0, sizeof(int)), "svs_tvl1_plan_create");
   if (st) { svs_tvl1_plan_destroy(P); return st; }
   // step-size schedule within a warp (tvl13d.py:208-211 reset, :240-249 update, host float64),
   // each value rounded to float as torch and pybind do.
@@ -926,7 +779,8 @@ svs_status svs_tvl1_plan_destroy(svs_plan* P) {
   if (P->cap_stream) cudaStreamDestroy(P->cap_stream);
   for (auto* t : P->d_tiles) cudaFree(t);
   cudaFree(P->d_descs); cudaFree(P->d_raw); cudaFree(P->d_uout); cudaFree(P->d_umed);
-  cudaFree(P->d_pout); cudaFree(P->d_uinit); cudaFree(P->d_pinit);
+  cudaFree(P->d_pout); cudaFree(P->d_uinit); cudaFree(P->d_pinit); cudaFree(P->d_maps);
+  cudaFree(P->d_status);
   cudaFree(P->arena);
   delete P;
   return SVS_OK;
@@ -957,7 +811,6 @@ svs_status svs_tvl1_solve_batch(svs_plan* P, const svs_pair_desc* pairs, int num
   warm = warm && P->levels == 1;
   cudaStream_t s = stream;
   svs_status st = SVS_OK;
-  // inputs -> plan buffers (one copy each)
   for (int i = 0; i < num_pairs && !st; ++i) {
     const size_t b = (size_t)P->h_descs[i].n * sizeof(float);
     st = check_cuda(cudaMemcpyAsync(P->raw[2 * i], pairs[i].I0, b, cudaMemcpyDeviceToDevice, s), "solve: input copy");
@@ -980,12 +833,10 @@ svs_status svs_tvl1_solve_batch(svs_plan* P, const svs_pair_desc* pairs, int num
   }
   P->warm = warm;
   if (P->tiles_built_for != P->tile_id) {
-    build_tiles(*P, P->tile_id);
-    st = upload_tiles(*P);
+    st = setup_tiles(*P);
     if (st) return st;
     P->tiles_built_for = P->tile_id;
   }
-  // the graph: captured once per (tile, warm start, want_p) configuration
   if (!P->exec || P->graph_tile != P->tile_id || P->graph_warm != warm || P->graph_want_p != want_p) {
     if (P->exec) { cudaGraphExecDestroy(P->exec); P->exec = nullptr; }
     cudaGraph_t g = nullptr;
@@ -1021,25 +872,29 @@ svs_status svs_tvl1_bench_iterations(svs_plan* P, int level, int count, svs_stre
   SVS_REQUIRE(level >= 0 && level < P->levels, "svs_tvl1_bench_iterations: bad level");
   SVS_REQUIRE(count >= 0, "svs_tvl1_bench_iterations: bad count");
   SVS_REQUIRE(P->tiles_built_for == P->tile_id, "svs_tvl1_bench_iterations: run a solve first");
-  const int tid = P->tile_id > 0 ? P->tile_id : auto_tile(*P, level);
   int cur = 0;
   for (int i = 0; i < count; ++i) {
-    IterArgs a;
     const int it = P->prm.max_outer_iterations > 0 ? i % P->prm.max_outer_iterations : 0;
-    a.sigma = P->sig_sched.empty() ? 0.5f : P->sig_sched[it];
-    a.tau = P->tau_sched.empty() ? 0.5f : P->tau_sched[it];
-    a.factor = a.tau * P->prm.weight_matching;
-    a.wtv = P->prm.weight_tv;
-    a.src = cur;
-    a.bdry = P->prm.boundary;
-    if (P->prm.storage == SVS_STORAGE_BF16) launch_iter_shape<__nv_bfloat16>(*P, level, tid, a, stream);
-    else if (P->prm.storage == SVS_STORAGE_F16) launch_iter_shape<__half>(*P, level, tid, a, stream);
-    else launch_iter_shape<float>(*P, level, tid, a, stream);
+    const IterArgs a = iter_args(*P, it, cur);
+    iter_dispatch(*P, nullptr, level, P->level_tile[level], 1, &a, stream);
     cur ^= 1;
   }
   return check_launch("svs_tvl1_bench_iterations", (uint64_t)count);
 }
 
 uint64_t svs_tvl1_plan_graph_kernels(const svs_plan* P) { return P ? P->graph_kernels : 0; }
+
+int svs_tvl1_plan_level_tile(const svs_plan* P, int level) {
+  return (P && level >= 0 && level < (int)P->level_tile.size()) ? P->level_tile[level] : 0;
+}
+
+svs_status svs_tvl1_plan_check(svs_plan* P) {
+  SVS_REQUIRE(P, "svs_tvl1_plan_check: null plan");
+  int flags = 0;
+  svs_status st = check_cuda(cudaMemcpy(&flags, P->d_status, sizeof(int), cudaMemcpyDeviceToHost), "svs_tvl1_plan_check");
+  if (st) return st;
+  if (flags & SVS_DEV_TIMEOUT) return fail(SVS_ERR_TIMEOUT, "a pipeline wait in the iterate kernel timed out; results are invalid");
+  return SVS_OK;
+}
 
 }  // extern "C"

@@ -63,6 +63,14 @@ class SolverPlan:
         with torch.cuda.device(self.device):
             check(_lib.lib().svs_tvl1_bench_iterations(self._h, int(level), int(count), s))
 
+    def check(self) -> None:
+        """Raise if a bounded pipeline wait inside an iterate kernel gave up (synchronizes)."""
+        with torch.cuda.device(self.device):
+            check(_lib.lib().svs_tvl1_plan_check(self._h))
+
+    def level_tiles(self):
+        return [int(_lib.lib().svs_tvl1_plan_level_tile(self._h, l)) for l in range(8)]
+
     @property
     def graph_kernels(self) -> int:
         return int(_lib.lib().svs_tvl1_plan_graph_kernels(self._h))

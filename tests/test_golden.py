@@ -1,0 +1,176 @@
+"""Parity against the reference itself: fixtures under tests/golden/ were produced by the
+reference's own compiled extension (tests/golden/make_golden_ref.py) on seeded inputs.
+
+CPU tests pin the oracle to those fixtures; GPU tests pin the libsvsflow kernels to them."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+INTERP = ["NEAREST", "LINEAR", "CUBIC_HERMITESPLINE"]
+BDRY = ["NEAREST", "MIRROR", "REFLECT"]
+
+
+def load(name):
+    path = os.path.join(GOLDEN, name)
+    if not os.path.exists(path):
+        pytest.fail(f"golden fixture missing: {path}")
+    return np.load(path)
+
+
+def op_cases(o, d):
+    """(name, oracle value) for every per-operator fixture."""
+    b, v, m = d["in_b"], d["in_v"], d["in_m"]
+    SH = b.shape
+    out = []
+    for name, L in (("dofs", tuple(s - 1 for s in SH)), ("fixed", (1.0, 2.0, 3.0))):
+        h = tuple(o.mesh_spacing(n, l) for n, l in zip(SH, L))
+        for bd in BDRY:
+            out += [(f"nabla_fwd_{name}_{bd}", lambda h=h, bd=bd: o.nabla_forward(b, h, bd)),
+                    (f"nabla_fwd_vf_{name}_{bd}", lambda h=h, bd=bd: o.nabla_forward_vf(v, h, bd)),
+                    (f"nabla_bwd_{name}_{bd}", lambda h=h, bd=bd: o.nabla_backward(v, h, bd)),
+                    (f"nabla_bwd_vf_{name}_{bd}", lambda h=h, bd=bd: o.nabla_backward_vf(m, h, bd))]
+    out += [("aniso_s", lambda: o.aniso_tangents(d["in_g"], 5.0, 0.5)[0]),
+            ("aniso_n", lambda: o.aniso_tangents(d["in_g"], 5.0, 0.5)[1]),
+            ("aniso_t1", lambda: o.aniso_tangents(d["in_g"], 5.0, 0.5)[2]),
+            ("aniso_t2", lambda: o.aniso_tangents(d["in_g"], 5.0, 0.5)[3]),
+            ("aniso_apply", lambda: o.aniso_apply(m, d["aniso_s"], d["aniso_n"], d["aniso_t1"])),
+            ("prox_dual", lambda: o.prox_dual(d["in_dv"], 0.025)),
+            ("prox_primal", lambda: o.prox_primal(v, 0.37, 1.0, d["in_rho"], d["in_gw"]))]
+    phi, go = d["in_phi"], d["in_gout"]
+    for it in INTERP:
+        for bd in BDRY:
+            out += [(f"warp_{it}_{bd}", lambda it=it, bd=bd: o.warp(b, phi, interp=it, bdry=bd)),
+                    (f"warp_vf_{it}_{bd}", lambda it=it, bd=bd: o.warp(v, phi, interp=it, bdry=bd)),
+                    (f"warp_bwd_u_{it}_{bd}", lambda it=it, bd=bd: o.warp_backward(b, phi, go, interp=it, bdry=bd)[0]),
+                    (f"warp_bwd_phi_{it}_{bd}", lambda it=it, bd=bd: o.warp_backward(b, phi, go, interp=it, bdry=bd)[1])]
+    for it in INTERP:
+        out += [(f"warp_cnn_{it}", lambda it=it: o.warp_cnn(d["in_cnn_m"], d["in_cnn_phi"], interp=it)),
+                (f"restrict_{it}", lambda it=it: o.prolongate(b, (6, 8, 10), (4, 5, 6), (3, 4, 5), interp=it)),
+                (f"prolong_vf_{it}", lambda it=it: o.prolongate(np.ascontiguousarray(v[:4, :5, :6]), (3, 4, 5), SH, (6, 8, 10), interp=it)),
+                (f"prolong_mf_{it}", lambda it=it: o.prolongate(np.ascontiguousarray(m[:4, :5, :6]), (3, 4, 5), SH, (6, 8, 10), interp=it))]
+    return out
+
+
+def test_oracle_matches_reference_operators(oracle):
+    d = load("ref_ops.npz")
+    bad = []
+    for name, fn in op_cases(oracle, d):
+        ref = d[name]
+        got = fn()
+        # tolerance: float32 rounding of the reference's fused multiply-adds (cubic weights,
+        # atomic accumulation order in the backward scatter)
+        tol = 5e-6 * max(1.0, float(np.abs(ref).max()))
+        if "bwd_u" in name:
+            tol *= 4
+        err = float(np.abs(got - ref).max())
+        if not err <= tol:
+            bad.append((name, err))
+        assert np.abs(ref).max() > 0 or name.startswith("warp_bwd_phi_NEAREST"), f"{name}: reference produced zeros"
+    assert not bad, bad
+
+
+def epe(a, b):
+    return np.sqrt(((np.asarray(a, np.float64) - np.asarray(b, np.float64)) ** 2).sum(-1))
+
+
+@pytest.mark.slow
+def test_oracle_solver_matches_reference_solver(oracle):
+    d = load("ref_solve32.npz")
+    u, _ = oracle.tvl1_compute(d["I0"], d["I1"], oracle.SolverParams(), dtype=np.float32)
+    for key in ("u", "u_notf32"):
+        e = epe(u, d[key])
+        assert e.mean() <= 0.05, (key, e.mean())
+        assert np.percentile(e, 99) <= 0.25, (key, np.percentile(e, 99))
+
+
+def test_oracle_masks_match_reference(oracle):
+    d = load("ref_masks.npz")
+    fwd, bwd = oracle.propagate_masks(d["m0"], d["mT"], d["ff"], d["bf"])
+    ref_f, ref_b = d["fwd"][:, 0], d["bwd"][:, 0]
+    for t in range(fwd.shape[0]):
+        assert oracle.dice(fwd[t], ref_f[t]) >= 0.99
+        assert oracle.dice(bwd[t], ref_b[t]) >= 0.99
+
+
+@pytest.mark.gpu
+def test_kernels_match_reference_operators(cuda):
+    from singleventriclesegmentation_b200 import opticalFlow as of
+    from singleventriclesegmentation_b200.flow_utils import apply_median_filter  # noqa: F401
+    d = load("ref_ops.npz")
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device="cuda")
+    N = lambda t: t.cpu().numpy()
+    b, v, m = d["in_b"], d["in_v"], d["in_m"]
+    SH = b.shape
+    got = {}
+    for name, L in (("dofs", tuple(s - 1 for s in SH)), ("fixed", (1.0, 2.0, 3.0))):
+        mesh = of.MeshInfo3D(*SH, *L)
+        for bd in BDRY:
+            op = of.Nabla3D_CD(mesh, getattr(of.BoundaryType, "BOUNDARY_" + bd))
+            got[f"nabla_fwd_{name}_{bd}"] = N(op.forward(T(b)))
+            got[f"nabla_fwd_vf_{name}_{bd}"] = N(op.forwardVectorField(T(v)))
+            got[f"nabla_bwd_{name}_{bd}"] = N(op.backward(T(v)))
+            got[f"nabla_bwd_vf_{name}_{bd}"] = N(op.backwardVectorField(T(m)))
+    mesh = of.MeshInfo3D(*SH, *(s - 1 for s in SH))
+    an = of.AnisotropicNabla3D(mesh, 5.0, 0.5)
+    tv = an.computeTangentVecs(T(d["in_g"]))
+    for k, t in zip(("aniso_s", "aniso_n", "aniso_t1", "aniso_t2"), tv):
+        got[k] = N(t)
+    got["aniso_apply"] = N(an.forwardVectorField(T(m), *tv))
+    got["prox_dual"] = N(of.TVL1OF3D_proxDual(T(d["in_dv"]), 0.5, 0.025, mesh))
+    got["prox_primal"] = N(of.TVL1OF3D_proxPrimal(T(v), 0.37, 1.0, T(d["in_rho"]), T(d["in_gw"]), mesh))
+    for it in INTERP:
+        for bd in BDRY:
+            w = of.Warping3D(mesh, getattr(of.InterpolationType, "INTERPOLATE_" + it), getattr(of.BoundaryType, "BOUNDARY_" + bd))
+            got[f"warp_{it}_{bd}"] = N(w.forward(T(b), T(d["in_phi"])))
+            got[f"warp_vf_{it}_{bd}"] = N(w.forwardVectorField(T(v), T(d["in_phi"])))
+            gu, gp = w.backward(T(b), T(d["in_phi"]), T(d["in_gout"]))
+            got[f"warp_bwd_u_{it}_{bd}"], got[f"warp_bwd_phi_{it}_{bd}"] = N(gu), N(gp)
+    small = (4, 5, 6)
+    mesh_s = of.MeshInfo3D(*small, *(s - 1 for s in small))
+    for it in INTERP:
+        ie = getattr(of.InterpolationType, "INTERPOLATE_" + it)
+        got[f"warp_cnn_{it}"] = N(of.WarpingCNN3D(mesh, ie, of.BoundaryType.BOUNDARY_MIRROR).forward(T(d["in_cnn_m"]), T(d["in_cnn_phi"])))
+        got[f"restrict_{it}"] = N(of.Prolongation3D(mesh, mesh_s, ie, of.BoundaryType.BOUNDARY_MIRROR).forward(T(b)))
+        up = of.Prolongation3D(mesh_s, mesh, ie, of.BoundaryType.BOUNDARY_MIRROR)
+        got[f"prolong_vf_{it}"] = N(up.forwardVectorField(T(v[:4, :5, :6])))
+        got[f"prolong_mf_{it}"] = N(up.forwardMatrixField(T(m[:4, :5, :6])))
+    bad = []
+    for k, g in got.items():
+        ref = d[k]
+        tol = 5e-6 * max(1.0, float(np.abs(ref).max())) * (4 if "bwd_u" in k else 1)
+        err = float(np.abs(g - ref).max())
+        if not err <= tol:
+            bad.append((k, err))
+    assert not bad, bad
+
+
+@pytest.mark.gpu
+def test_fused_solver_matches_reference_solver(cuda, oracle):
+    from singleventriclesegmentation_b200.tvl13d import TVL13DOpticalFlow
+    d = load("ref_solve32.npz")
+    P = oracle.SolverParams()
+    s = TVL13DOpticalFlow(P.num_scales, P.max_warps, P.max_outer_iterations, P.weight_matching, P.weight_tv,
+                          P.primaldual_algorithm_type, P.primaldual_algorithm_params, P.use_anisotropic_diff,
+                          P.anisotropic_diff_params, P.use_gaussian_blur, P.gaussian_blur_sigma,
+                          P.interpolation_type, P.boundary_type, P.length_type, P.length, torch.device("cuda"))
+    u, _ = s.compute(torch.from_numpy(d["I0"]).cuda(), torch.from_numpy(d["I1"]).cuda())
+    for key in ("u", "u_notf32"):
+        e = epe(u.cpu().numpy(), d[key])
+        print(key, "mean EPE", e.mean(), "p99", np.percentile(e, 99), "max", e.max())
+        assert e.mean() <= 0.05, (key, e.mean())
+        assert np.percentile(e, 99) <= 0.25
+
+
+@pytest.mark.gpu
+def test_masks_match_reference(cuda):
+    from singleventriclesegmentation_b200.warping import Warp, dice, propagate
+    d = load("ref_masks.npz")
+    w = Warp("CUBIC_HERMITESPLINE", "MIRROR", "numDofs", (1, 1, 1))
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device="cuda")
+    fwd, bwd = propagate(w, T(d["m0"])[None, None], T(d["mT"])[None, None], T(d["ff"]), T(d["bf"]))
+    for t in range(fwd.shape[0]):
+        assert dice(fwd[t, 0], T(d["fwd"][t, 0])) >= 0.99
+        assert dice(bwd[t, 0], T(d["bwd"][t, 0])) >= 0.99
