@@ -45,8 +45,16 @@ typedef enum {
 enum { SVS_BOUNDARY_NEAREST = 0, SVS_BOUNDARY_MIRROR = 1, SVS_BOUNDARY_REFLECT = 2 };
 /* svs/src/coreDefines.h:94-100 */
 enum { SVS_INTERPOLATE_NEAREST = 0, SVS_INTERPOLATE_LINEAR = 1, SVS_INTERPOLATE_CUBIC_HERMITESPLINE = 2 };
-/* storage precision of the fused solver's state (arithmetic is always FP32) */
-enum { SVS_STORAGE_F32 = 0, SVS_STORAGE_BF16 = 1, SVS_STORAGE_F16 = 2 };
+/* storage precision of the fused solver's iteration state (arithmetic is always FP32):
+ * all fields F32; all fields BF16 or FP16; or the flow u in F32 with the dual field, the tensor
+ * D and the linearisation (rho_c, warped gradient) in BF16 / FP16. */
+enum {
+  SVS_STORAGE_F32 = 0,
+  SVS_STORAGE_BF16 = 1,
+  SVS_STORAGE_F16 = 2,
+  SVS_STORAGE_BF16_FLOW32 = 3,
+  SVS_STORAGE_F16_FLOW32 = 4
+};
 
 const char* svs_last_error(void);
 int svs_version(void);
@@ -177,7 +185,7 @@ svs_status svs_tvl1_plan_destroy(svs_plan* plan);
 /* Bytes of device memory the plan holds. */
 size_t svs_tvl1_plan_device_bytes(const svs_plan* plan);
 /* Select the iterate-kernel variant (0 = automatic) for later solves; SVS_ERR_INVALID_ARG for an
- * unknown id. Variants 1-5 are TMA pipelines (32x8/5 stages, 32x8/4, 64x4/4, 16x16/4, 32x16/4),
+ * unknown id. Variants 1-5 are TMA pipelines (tile x prefetch distance: 32x8/2, 32x8/3, 64x4/2, 16x16/2, 32x16/2),
  * 6-8 plain-load forms (32x8, 32x4, 16x16). Used by the autotuner. */
 svs_status svs_tvl1_plan_set_tile(svs_plan* plan, int tile_id);
 int svs_tvl1_num_tiles(void);

@@ -21,7 +21,8 @@ STATUS_NAMES = {0: "SVS_OK", 1: "SVS_ERR_INVALID_ARG", 2: "SVS_ERR_OUT_OF_MEMORY
                 3: "SVS_ERR_LAUNCH", 4: "SVS_ERR_TIMEOUT", 5: "SVS_ERR_UNSUPPORTED",
                 6: "SVS_ERR_CUDA"}
 
-STORAGE = {"f32": 0, "float32": 0, "bf16": 1, "bfloat16": 1, "f16": 2, "float16": 2}
+STORAGE = {"f32": 0, "float32": 0, "bf16": 1, "bfloat16": 1, "f16": 2, "float16": 2,
+           "bf16-flow32": 3, "f16-flow32": 4}
 
 
 class TVL1Params(ctypes.Structure):

@@ -2,8 +2,8 @@
 // iteration, in two forms:
 //   iterate_kernel      plain loads, one z-plane of each field per step, state in registers;
 //   iterate_tma_kernel  a multi-stage TMA pipeline: one thread issues cp.async.bulk.tensor
-//                       loads of whole plane tiles (u, p, D, rc, gw) several planes ahead into a
-//                       shared-memory ring, completion tracked by mbarriers.
+//                       loads of whole plane tiles (u, p, D, rc, gw) DIST planes ahead into
+//                       shared-memory rings, completion tracked by mbarriers.
 // Both march a TX x TY column tile along z. Thread (tx, ty) of the (TX+2) x (TY+2) block owns
 // column (x0-1+tx, y0-1+ty) of the "dual region" (tile plus a one-voxel x/y halo). At plane k:
 //   dual:   on the dual region minus its 4 corners, p_new(k) = proj(p + sigma D grad u) and
@@ -12,12 +12,46 @@
 //           published rows of plane j and the registers of planes j-1 and j+1, then
 //           u_new(j) = prox_primal(u - tau div).
 // Halo duals are recomputed by neighbouring tiles, so the tiles of one launch are independent
-// (u and p are ping-pong buffers). The arithmetic of both forms is identical.
+// (u and p are ping-pong buffers). The flow u is stored as SU, everything else as SP.
+//
+// Difference stencils use per-position coefficients (prev, cur, next) instead of boundary
+// branches; with h = 1 the result is bitwise the reference's expression:
+//   forward  0.5*(next - prev)/h               differentialOps.cu:540-655 (one-sided at faces
+//                                              for NEAREST/REFLECT, zero for MIRROR)
+//   adjoint  MIRROR  i>1&&i<N-2: 0.5(prev-next); i>1: 0.5 prev; else -0.5 next
+//            others  0<i<N-1: 0.5(prev-next); i=N-1: 0.5(prev+cur); i=0: 0.5(-cur-next)
+//                                              differentialOps.cu:658-1039 (then /h)
 #pragma once
 
 #include "svs_state.cuh"
 
 namespace svs {
+
+struct Stencil3 {
+  float m, c, p;
+};
+
+__device__ __forceinline__ Stencil3 fwd_coef(int i, int n, int bdry, float h) {
+  const float a = 0.5f / h;
+  if (i > 0 && i < n - 1) return {-a, 0.f, a};
+  if (bdry == SVS_BOUNDARY_MIRROR) return {0.f, 0.f, 0.f};
+  if (i > 0) return {-a, a, 0.f};  // i == n-1
+  return {0.f, -a, a};             // i == 0
+}
+
+__device__ __forceinline__ Stencil3 adj_coef(int i, int n, int bdry, float ih) {
+  const float a = 0.5f * ih;
+  if (bdry == SVS_BOUNDARY_MIRROR) {
+    if (i > 1) return (i < n - 2) ? Stencil3{a, 0.f, -a} : Stencil3{a, 0.f, 0.f};
+    return {0.f, 0.f, -a};
+  }
+  if (i > 0) return (i < n - 1) ? Stencil3{a, 0.f, -a} : Stencil3{a, a, 0.f};
+  return {0.f, -a, -a};
+}
+
+__device__ __forceinline__ float apply3(const Stencil3& s, float prev, float cur, float next) {
+  return fmaf(s.p, next, fmaf(s.c, cur, s.m * prev));
+}
 
 // Dual update of one flow component at one voxel, tvl13d.py:215-222 with
 // opticalFlowOps.cu:179-208: v = p + sigma D g; p_new = v / max(1, |v| / weight_tv), written as
@@ -62,7 +96,7 @@ __device__ __forceinline__ void primal_voxel(const float u[3], const float div[3
 }
 
 // ------------------------------------------------------------------------ plain-load form
-template <typename S, int TX, int TY>
+template <typename SU, typename SP, int TX, int TY>
 __global__ void __launch_bounds__((TX + 2) * (TY + 2))
 iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, IterArgs a) {
   constexpr int PX = TX + 2, PY = TY + 2, UX = TX + 4, UY = TY + 4;
@@ -73,18 +107,16 @@ iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, I
   const Tile T = tiles[blockIdx.x];
   const Desc& Dg = descs[T.desc];
   const int nz = Dg.nz, ny = Dg.ny, nx = Dg.nx;
-  const float ihz = 1.0f / Dg.hz, ihy = 1.0f / Dg.hy, ihx = 1.0f / Dg.hx;
-  const float hz = Dg.hz, hy = Dg.hy, hx = Dg.hx;
-  const long long cs = Dg.cs;
-  const long long plane = (long long)Dg.pitch * ny;
+  const int cs = (int)Dg.cs;
+  const int plane = Dg.pitch * ny;
   const int z0 = T.z0z1 & 0xffff, z1 = T.z0z1 >> 16;
-  const S* __restrict__ u_src = reinterpret_cast<const S*>(Dg.u[a.src]);
-  const S* __restrict__ p_src = reinterpret_cast<const S*>(Dg.p[a.src]);
-  S* __restrict__ u_dst = reinterpret_cast<S*>(Dg.u[a.src ^ 1]);
-  S* __restrict__ p_dst = reinterpret_cast<S*>(Dg.p[a.src ^ 1]);
-  const S* __restrict__ Dm = reinterpret_cast<const S*>(Dg.D);
-  const S* __restrict__ rcm = reinterpret_cast<const S*>(Dg.rc);
-  const S* __restrict__ gwm = reinterpret_cast<const S*>(Dg.gw);
+  const SU* __restrict__ u_src = reinterpret_cast<const SU*>(Dg.u[a.src]);
+  const SP* __restrict__ p_src = reinterpret_cast<const SP*>(Dg.p[a.src]);
+  SU* __restrict__ u_dst = reinterpret_cast<SU*>(Dg.u[a.src ^ 1]);
+  SP* __restrict__ p_dst = reinterpret_cast<SP*>(Dg.p[a.src ^ 1]);
+  const SP* __restrict__ Dm = reinterpret_cast<const SP*>(Dg.D);
+  const SP* __restrict__ rcm = reinterpret_cast<const SP*>(Dg.rc);
+  const SP* __restrict__ gwm = reinterpret_cast<const SP*>(Dg.gw);
 
   const int tid = threadIdx.x;
   const int tx = tid % PX, ty = tid / PX;
@@ -93,7 +125,11 @@ iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, I
   const bool corner = (tx == 0 || tx == PX - 1) && (ty == 0 || ty == PY - 1);
   const bool dual_on = in_dom && !corner;
   const bool interior = in_dom && tx >= 1 && tx <= TX && ty >= 1 && ty <= TY;
-  const long long col = (long long)gy * Dg.pitch + gx;
+  const int col = gy * Dg.pitch + gx;
+  const int bdry = a.bdry;
+  const Stencil3 fx = fwd_coef(gx, nx, bdry, Dg.hx), fy = fwd_coef(gy, ny, bdry, Dg.hy);
+  const Stencil3 ax = adj_coef(gx, nx, bdry, 1.0f / Dg.hx), ay = adj_coef(gy, ny, bdry, 1.0f / Dg.hy);
+  const float ihz = 1.0f / Dg.hz;
 
   int rx = -1, ry = -1;
   if (tid < NRING) {
@@ -105,40 +141,39 @@ iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, I
   }
   const int rgx = T.x0 - 2 + rx, rgy = T.y0 - 2 + ry;
   const bool ring_on = tid < NRING && rgx >= 0 && rgx < nx && rgy >= 0 && rgy < ny;
-  const long long rcol = (long long)rgy * Dg.pitch + rgx;
+  const int rcol = rgy * Dg.pitch + rgx;
 
   const int kb = max(z0 - 1, 0), ke = min(z1, nz - 1);
   float um[3] = {0.f, 0.f, 0.f}, uc[3] = {0.f, 0.f, 0.f}, up[3] = {0.f, 0.f, 0.f};
   if (in_dom) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      if (kb >= 1) um[c] = Store<S>::ld(u_src + c * cs + (kb - 1) * plane + col);
-      uc[c] = Store<S>::ld(u_src + c * cs + kb * plane + col);
-      if (kb + 1 < nz) up[c] = Store<S>::ld(u_src + c * cs + (kb + 1) * plane + col);
+      if (kb >= 1) um[c] = Store<SU>::ld(u_src + c * cs + (kb - 1) * plane + col);
+      uc[c] = Store<SU>::ld(u_src + c * cs + kb * plane + col);
+      if (kb + 1 < nz) up[c] = Store<SU>::ld(u_src + c * cs + (kb + 1) * plane + col);
     }
   }
   float qzmm[3] = {0.f, 0.f, 0.f}, qzm[3] = {0.f, 0.f, 0.f}, qzc[3] = {0.f, 0.f, 0.f};
   const float wtv2 = a.wtv * a.wtv;
-  const int bdry = a.bdry;
 
   for (int k = kb; k <= ke; ++k) {
     const int slot = k & 1;
     float pk[9], Dk[6];
     if (dual_on) {
-      const long long o = k * plane + col;
+      const int o = k * plane + col;
 #pragma unroll
-      for (int c = 0; c < 9; ++c) pk[c] = Store<S>::ld(p_src + c * cs + o);
+      for (int c = 0; c < 9; ++c) pk[c] = Store<SP>::ld(p_src + c * cs + o);
 #pragma unroll
-      for (int c = 0; c < 6; ++c) Dk[c] = Store<S>::ld(Dm + c * cs + o);
+      for (int c = 0; c < 6; ++c) Dk[c] = Store<SP>::ld(Dm + c * cs + o);
     }
     const int j = k - 1;
     const bool primal_on = interior && j >= z0 && j < z1;
     float rcj = 0.f, gj[3] = {0.f, 0.f, 0.f};
     if (primal_on) {
-      const long long o = j * plane + col;
-      rcj = Store<S>::ld(rcm + o);
+      const int o = j * plane + col;
+      rcj = Store<SP>::ld(rcm + o);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) gj[c] = Store<S>::ld(gwm + c * cs + o);
+      for (int c = 0; c < 3; ++c) gj[c] = Store<SP>::ld(gwm + c * cs + o);
     }
     if (in_dom) {
 #pragma unroll
@@ -146,21 +181,22 @@ iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, I
     }
     if (ring_on) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) su[slot][c][ry][rx] = Store<S>::ld(u_src + c * cs + k * plane + rcol);
+      for (int c = 0; c < 3; ++c) su[slot][c][ry][rx] = Store<SU>::ld(u_src + c * cs + k * plane + rcol);
     }
     __syncthreads();
     if (dual_on) {
+      const Stencil3 fz = fwd_coef(k, nz, bdry, Dg.hz);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const float ex = fwd_axis(su[slot][c][ty + 1][tx], uc[c], su[slot][c][ty + 1][tx + 2], gx, nx, bdry, hx);
-        const float ey = fwd_axis(su[slot][c][ty][tx + 1], uc[c], su[slot][c][ty + 2][tx + 1], gy, ny, bdry, hy);
-        const float ez = fwd_axis(um[c], uc[c], up[c], k, nz, bdry, hz);
+        const float ex = apply3(fx, su[slot][c][ty + 1][tx], uc[c], su[slot][c][ty + 1][tx + 2]);
+        const float ey = apply3(fy, su[slot][c][ty][tx + 1], uc[c], su[slot][c][ty + 2][tx + 1]);
+        const float ez = apply3(fz, um[c], uc[c], up[c]);
         dual_row(Dk, ex, ey, ez, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2], a.sigma, a.wtv, wtv2);
       }
       if (interior && k >= z0 && k < z1) {
-        const long long o = k * plane + col;
+        const int o = k * plane + col;
 #pragma unroll
-        for (int c = 0; c < 9; ++c) Store<S>::st(p_dst + c * cs + o, pk[c]);
+        for (int c = 0; c < 9; ++c) Store<SP>::st(p_dst + c * cs + o, pk[c]);
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -171,18 +207,18 @@ iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, I
     }
     if (primal_on) {
       const int ps = slot ^ 1;
+      const Stencil3 az = adj_coef(j, nz, bdry, ihz);
       float div[3], un[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const float ax = adj_axis(sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1], gx, nx, bdry);
-        const float ay = adj_axis(sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx], gy, ny, bdry);
-        const float az = adj_axis(qzmm[c], qzm[c], qzc[c], j, nz, bdry);
-        div[c] = (ax * ihx + ay * ihy) + az * ihz;
+        const float dx = apply3(ax, sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1]);
+        const float dy = apply3(ay, sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx]);
+        div[c] = (dx + dy) + apply3(az, qzmm[c], qzm[c], qzc[c]);
       }
       primal_voxel(um, div, a.tau, a.factor, rcj, gj, un);
-      const long long o = j * plane + col;
+      const int o = j * plane + col;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) Store<S>::st(u_dst + c * cs + o, un[c]);
+      for (int c = 0; c < 3; ++c) Store<SU>::st(u_dst + c * cs + o, un[c]);
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -194,7 +230,7 @@ iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, I
     }
     if (in_dom && k + 2 < nz) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) up[c] = Store<S>::ld(u_src + c * cs + (k + 2) * plane + col);
+      for (int c = 0; c < 3; ++c) up[c] = Store<SU>::ld(u_src + c * cs + (k + 2) * plane + col);
     }
   }
   if (z1 >= nz) {
@@ -202,21 +238,21 @@ iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, I
     const int j = nz - 1;
     if (interior && j >= z0) {
       const int ps = j & 1;
-      const long long o = j * plane + col;
+      const int o = j * plane + col;
+      const Stencil3 az = adj_coef(j, nz, bdry, ihz);
       float gj[3], div[3], un[3];
-      const float rcj = Store<S>::ld(rcm + o);
+      const float rcj = Store<SP>::ld(rcm + o);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) gj[c] = Store<S>::ld(gwm + c * cs + o);
+      for (int c = 0; c < 3; ++c) gj[c] = Store<SP>::ld(gwm + c * cs + o);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const float ax = adj_axis(sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1], gx, nx, bdry);
-        const float ay = adj_axis(sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx], gy, ny, bdry);
-        const float az = adj_axis(qzmm[c], qzm[c], 0.f, j, nz, bdry);
-        div[c] = (ax * ihx + ay * ihy) + az * ihz;
+        const float dx = apply3(ax, sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1]);
+        const float dy = apply3(ay, sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx]);
+        div[c] = (dx + dy) + apply3(az, qzmm[c], qzm[c], 0.f);
       }
       primal_voxel(um, div, a.tau, a.factor, rcj, gj, un);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) Store<S>::st(u_dst + c * cs + o, un[c]);
+      for (int c = 0; c < 3; ++c) Store<SU>::st(u_dst + c * cs + o, un[c]);
     }
   }
 }
@@ -272,44 +308,54 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, u
 
 __host__ __device__ constexpr int round_up_c(int v, int m) { return (v + m - 1) / m * m; }
 
-// Shared-memory geometry of the TMA form for storage S and tile TX x TY with NSTG stages.
-template <typename S, int TX, int TY, int NSTG>
+// Shared-memory geometry of the TMA form: flow stored as SU, the rest as SP, tile TX x TY,
+// prefetch distance DIST planes.
+//   u ring    DIST+2 slots: planes k-1, k, k+1 are read at step k;
+//   p/D ring  DIST slots:   plane k is read only by the dual of step k;
+//   rc/gw     DIST+2 slots: plane j = k-1 is read after the barrier of step k;
+//   mbarrier  one per plane, DIST+2 slots.
+// Plane k+DIST is issued after the barrier of step k, into the u/rc-gw slot of plane k-2 and the
+// p/D slot of plane k, all of which every thread has finished reading by then. The first plane
+// (k = kb-1, the z-neighbour of the first dual plane) carries u only.
+template <typename SU, typename SP, int TX, int TY, int DIST>
 struct TmaGeom {
-  static constexpr int ES = (int)sizeof(S);
-  static constexpr int A = 16 / ES;                       // 16-byte alignment in elements
+  static constexpr int ESU = (int)sizeof(SU), ESP = (int)sizeof(SP);
+  static constexpr int AU = 16 / ESU, AP = 16 / ESP;      // 16-byte alignment in elements
   static constexpr int PX = TX + 2, PY = TY + 2;
-  static constexpr int UXB = round_up_c(TX + A + 2, A);   // u box: x in [x0-A, x0-A+UXB)
-  static constexpr int PXB = round_up_c(TX + A + 1, A);   // p/D box: x in [x0-A, x0-A+PXB)
-  static constexpr int UYB = TY + 4, PYB = TY + 2;        // u box rows from y0-2, p/D from y0-1
-  static constexpr int U_TX = 3 * UYB * UXB * ES;
-  static constexpr int P_TX = 9 * PYB * PXB * ES;
-  static constexpr int D_TX = 6 * PYB * PXB * ES;
-  static constexpr int RC_TX = TY * TX * ES;
-  static constexpr int GW_TX = 3 * TY * TX * ES;
+  static constexpr int UXB = round_up_c(TX + AU + 2, AU);  // u box: x in [x0-AU, x0-AU+UXB)
+  static constexpr int PXB = round_up_c(TX + AP + 1, AP);  // p/D box: x in [x0-AP, x0-AP+PXB)
+  static constexpr int UYB = TY + 4, PYB = TY + 2;         // u rows from y0-2, p/D from y0-1
+  static constexpr int U_TX = 3 * UYB * UXB * ESU;
+  static constexpr int P_TX = 9 * PYB * PXB * ESP;
+  static constexpr int D_TX = 6 * PYB * PXB * ESP;
+  static constexpr int RC_TX = TY * TX * ESP;
+  static constexpr int GW_TX = 3 * TY * TX * ESP;
+  static constexpr int NU = DIST + 2, NPD = DIST, NR = DIST + 2, NB = DIST + 2;
+  static constexpr int U_SLOT = round_up_c(U_TX, 128);
+  static constexpr int P_SLOT = round_up_c(P_TX, 128);
+  static constexpr int D_SLOT = round_up_c(D_TX, 128);
+  static constexpr int RC_SLOT = round_up_c(RC_TX, 128);
+  static constexpr int GW_SLOT = round_up_c(GW_TX, 128);
   static constexpr int U_OFF = 0;
-  static constexpr int P_OFF = round_up_c(U_OFF + U_TX, 128);
-  static constexpr int D_OFF = round_up_c(P_OFF + P_TX, 128);
-  static constexpr int RC_OFF = round_up_c(D_OFF + D_TX, 128);
-  static constexpr int GW_OFF = round_up_c(RC_OFF + RC_TX, 128);
-  static constexpr int STAGE = round_up_c(GW_OFF + GW_TX, 128);
-  static constexpr int STAGE_TX = U_TX + P_TX + D_TX + RC_TX + GW_TX;
-  static constexpr int SQ_OFF = NSTG * STAGE;
+  static constexpr int PD_OFF = U_OFF + NU * U_SLOT;
+  static constexpr int PD_SLOT = P_SLOT + D_SLOT;
+  static constexpr int R_OFF = PD_OFF + NPD * PD_SLOT;
+  static constexpr int R_SLOT = RC_SLOT + GW_SLOT;
+  static constexpr int SQ_OFF = R_OFF + NR * R_SLOT;
   static constexpr int SQ_BYTES = 3 * 6 * PY * PX * 4;
   static constexpr int BAR_OFF = round_up_c(SQ_OFF + SQ_BYTES, 8);
-  static constexpr int SMEM = BAR_OFF + NSTG * 8;
+  static constexpr int SMEM = BAR_OFF + NB * 8;
+  static constexpr int FULL_TX = U_TX + P_TX + D_TX + RC_TX + GW_TX;
 };
 
-template <typename S, int TX, int TY, int NSTG>
+template <typename SU, typename SP, int TX, int TY, int DIST>
 __global__ void __launch_bounds__((TX + 2) * (TY + 2))
 iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs,
                    const TMaps* __restrict__ maps, IterArgs a, int* __restrict__ status) {
-  using G = TmaGeom<S, TX, TY, NSTG>;
-  constexpr int PX = G::PX, PY = G::PY, A = G::A, UXB = G::UXB, UYB = G::UYB, PXB = G::PXB,
-                PYB = G::PYB;
-  // Planes k-1, k, k+1 are read at step k; plane k+DIST is issued after the step's barrier into
-  // the slot of plane k-2. Step k waits for plane k+1, issued at step k+1-DIST: DIST >= 2.
-  static_assert(NSTG >= 4, "the TMA pipeline needs at least 4 stages");
-  constexpr int DIST = NSTG - 2;  // prefetch distance in planes
+  using G = TmaGeom<SU, SP, TX, TY, DIST>;
+  constexpr int PX = G::PX, PY = G::PY, AU = G::AU, AP = G::AP, UXB = G::UXB, UYB = G::UYB,
+                PXB = G::PXB, PYB = G::PYB;
+  static_assert(DIST >= 2, "step k waits for plane k+1, issued at step k+1-DIST");
   extern __shared__ __align__(128) unsigned char smem[];
   float(*sq)[6][PY][PX] = reinterpret_cast<float(*)[6][PY][PX]>(smem + G::SQ_OFF);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + G::BAR_OFF);
@@ -318,13 +364,11 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
   const Desc& Dg = descs[T.desc];
   const TMaps* M = maps + T.desc;
   const int nz = Dg.nz, ny = Dg.ny, nx = Dg.nx;
-  const float ihz = 1.0f / Dg.hz, ihy = 1.0f / Dg.hy, ihx = 1.0f / Dg.hx;
-  const float hz = Dg.hz, hy = Dg.hy, hx = Dg.hx;
-  const long long cs = Dg.cs;
-  const long long plane = (long long)Dg.pitch * ny;
+  const int cs = (int)Dg.cs;
+  const int plane = Dg.pitch * ny;
   const int z0 = T.z0z1 & 0xffff, z1 = T.z0z1 >> 16;
-  S* __restrict__ u_dst = reinterpret_cast<S*>(Dg.u[a.src ^ 1]);
-  S* __restrict__ p_dst = reinterpret_cast<S*>(Dg.p[a.src ^ 1]);
+  SU* __restrict__ u_dst = reinterpret_cast<SU*>(Dg.u[a.src ^ 1]);
+  SP* __restrict__ p_dst = reinterpret_cast<SP*>(Dg.p[a.src ^ 1]);
   const CUtensorMap* mu = &M->u[a.src];
   const CUtensorMap* mp = &M->p[a.src];
 
@@ -335,27 +379,41 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
   const bool corner = (tx == 0 || tx == PX - 1) && (ty == 0 || ty == PY - 1);
   const bool dual_on = in_dom && !corner;
   const bool interior = in_dom && tx >= 1 && tx <= TX && ty >= 1 && ty <= TY;
-  const long long col = (long long)gy * Dg.pitch + gx;
-  const int ux = tx + A - 1, uy = ty + 1;  // own column in the u box
-  const int px = tx + A - 1, py = ty;      // own column in the p/D boxes
+  const int col = gy * Dg.pitch + gx;
+  const int uo = (ty + 1) * UXB + (tx + AU - 1);  // own column in a u box component
+  const int po = ty * PXB + (tx + AP - 1);        // own column in a p/D box component
+  const int ro = (ty - 1) * TX + (tx - 1);        // own column in an rc/gw box (interior)
+  const int bdry = a.bdry;
+  const Stencil3 fx = fwd_coef(gx, nx, bdry, Dg.hx), fy = fwd_coef(gy, ny, bdry, Dg.hy);
+  const Stencil3 ax = adj_coef(gx, nx, bdry, 1.0f / Dg.hx), ay = adj_coef(gy, ny, bdry, 1.0f / Dg.hy);
+  const float ihz = 1.0f / Dg.hz, hz = Dg.hz;
 
   const int kb = max(z0 - 1, 0), ke = min(z1, nz - 1);
   const int pl = max(kb - 1, 0), ph = min(ke + 1, nz - 1);  // planes staged by this tile
-
-  auto stage = [&](int q) -> unsigned char* { return smem + ((q - pl) % NSTG) * G::STAGE; };
   auto issue = [&](int q) {
-    unsigned char* st = stage(q);
-    uint64_t* bar = bars + (q - pl) % NSTG;
-    mbar_arrive_expect_tx(bar, (uint32_t)G::STAGE_TX);
-    tma_load_4d(st + G::U_OFF, mu, bar, T.x0 - A, T.y0 - 2, q, 0);
-    tma_load_4d(st + G::P_OFF, mp, bar, T.x0 - A, T.y0 - 1, q, 0);
-    tma_load_4d(st + G::D_OFF, &M->D, bar, T.x0 - A, T.y0 - 1, q, 0);
-    tma_load_4d(st + G::RC_OFF, &M->rc, bar, T.x0, T.y0, q, 0);
-    tma_load_4d(st + G::GW_OFF, &M->gw, bar, T.x0, T.y0, q, 0);
+    const int r = q - pl;
+    uint64_t* bar = bars + r % G::NB;
+    unsigned char* U = smem + G::U_OFF + (r % G::NU) * G::U_SLOT;
+    if (q < kb) {
+      mbar_arrive_expect_tx(bar, (uint32_t)G::U_TX);
+      tma_load_4d(U, mu, bar, T.x0 - AU, T.y0 - 2, q, 0);
+      return;
+    }
+    unsigned char* PD = smem + G::PD_OFF + ((q - kb) % G::NPD) * G::PD_SLOT;
+    unsigned char* R = smem + G::R_OFF + ((q - kb) % G::NR) * G::R_SLOT;
+    mbar_arrive_expect_tx(bar, (uint32_t)G::FULL_TX);
+    tma_load_4d(U, mu, bar, T.x0 - AU, T.y0 - 2, q, 0);
+    tma_load_4d(PD, mp, bar, T.x0 - AP, T.y0 - 1, q, 0);
+    tma_load_4d(PD + G::P_SLOT, &M->D, bar, T.x0 - AP, T.y0 - 1, q, 0);
+    tma_load_4d(R, &M->rc, bar, T.x0, T.y0, q, 0);
+    tma_load_4d(R + G::RC_SLOT, &M->gw, bar, T.x0, T.y0, q, 0);
+  };
+  auto ubox = [&](int q) {
+    return reinterpret_cast<const SU*>(smem + G::U_OFF + ((q - pl) % G::NU) * G::U_SLOT);
   };
 
   if (tid == 0) {
-    for (int s = 0; s < NSTG; ++s) mbar_init(bars + s, 1);
+    for (int s = 0; s < G::NB; ++s) mbar_init(bars + s, 1);
     mbar_fence_init();
   }
   __syncthreads();
@@ -365,48 +423,47 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
     for (int q = pl; q <= last; ++q) issue(q);
     issued = last;
   }
-  int waited = pl - 1;  // every thread: planes <= waited are complete
+  int waited = pl - 1;  // planes <= waited are complete (per thread)
   bool bad = false;
-
-  auto uval = [&](int q, int c, int yy, int xx) -> float {
-    const S* U = reinterpret_cast<const S*>(stage(q) + G::U_OFF);
-    return Store<S>::sh(U + (c * UYB + yy) * UXB + xx);
-  };
 
   float qzmm[3] = {0.f, 0.f, 0.f}, qzm[3] = {0.f, 0.f, 0.f}, qzc[3] = {0.f, 0.f, 0.f};
   const float wtv2 = a.wtv * a.wtv;
-  const int bdry = a.bdry;
 
   for (int k = kb; k <= ke; ++k) {
     const int need = min(k + 1, ph);
     while (waited < need && !bad) {
       ++waited;
-      if (!mbar_wait(bars + (waited - pl) % NSTG, (uint32_t)(((waited - pl) / NSTG) & 1))) bad = true;
+      const int r = waited - pl;
+      if (!mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1))) bad = true;
     }
+    const int qs = k % 3;
     if (dual_on && !bad) {
-      const S* P = reinterpret_cast<const S*>(stage(k) + G::P_OFF);
-      const S* Dm = reinterpret_cast<const S*>(stage(k) + G::D_OFF);
+      const SU* Uk = ubox(k) + uo;
+      const SU* Um = (k - 1 >= pl) ? ubox(k - 1) + uo : Uk;  // coefficient 0 where absent
+      const SU* Up = (k + 1 <= ph) ? ubox(k + 1) + uo : Uk;
+      const unsigned char* PD = smem + G::PD_OFF + ((k - kb) % G::NPD) * G::PD_SLOT;
+      const SP* P = reinterpret_cast<const SP*>(PD) + po;
+      const SP* Dm = reinterpret_cast<const SP*>(PD + G::P_SLOT) + po;
+      const Stencil3 fz = fwd_coef(k, nz, bdry, hz);
       float pk[9], Dk[6];
 #pragma unroll
-      for (int c = 0; c < 9; ++c) pk[c] = Store<S>::sh(P + (c * PYB + py) * PXB + px);
+      for (int c = 0; c < 9; ++c) pk[c] = Store<SP>::sh(P + c * PYB * PXB);
 #pragma unroll
-      for (int c = 0; c < 6; ++c) Dk[c] = Store<S>::sh(Dm + (c * PYB + py) * PXB + px);
+      for (int c = 0; c < 6; ++c) Dk[c] = Store<SP>::sh(Dm + c * PYB * PXB);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const float uc = uval(k, c, uy, ux);
-        const float ex = fwd_axis(uval(k, c, uy, ux - 1), uc, uval(k, c, uy, ux + 1), gx, nx, bdry, hx);
-        const float ey = fwd_axis(uval(k, c, uy - 1, ux), uc, uval(k, c, uy + 1, ux), gy, ny, bdry, hy);
-        const float zm = (k - 1 >= pl) ? uval(k - 1, c, uy, ux) : 0.f;
-        const float zp = (k + 1 <= ph) ? uval(k + 1, c, uy, ux) : 0.f;
-        const float ez = fwd_axis(zm, uc, zp, k, nz, bdry, hz);
+        const SU* u = Uk + c * UYB * UXB;
+        const float uc = Store<SU>::sh(u);
+        const float ex = apply3(fx, Store<SU>::sh(u - 1), uc, Store<SU>::sh(u + 1));
+        const float ey = apply3(fy, Store<SU>::sh(u - UXB), uc, Store<SU>::sh(u + UXB));
+        const float ez = apply3(fz, Store<SU>::sh(Um + c * UYB * UXB), uc, Store<SU>::sh(Up + c * UYB * UXB));
         dual_row(Dk, ex, ey, ez, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2], a.sigma, a.wtv, wtv2);
       }
       if (interior && k >= z0 && k < z1) {
-        const long long o = k * plane + col;
+        SP* dst = p_dst + k * plane + col;
 #pragma unroll
-        for (int c = 0; c < 9; ++c) Store<S>::st(p_dst + c * cs + o, pk[c]);
+        for (int c = 0; c < 9; ++c) Store<SP>::st(dst + c * cs, pk[c]);
       }
-      const int qs = k % 3;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         sq[qs][c][ty][tx] = Dk[0] * pk[3 * c] + Dk[1] * pk[3 * c + 1] + Dk[2] * pk[3 * c + 2];
@@ -414,7 +471,7 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
         qzc[c] = Dk[2] * pk[3 * c] + Dk[4] * pk[3 * c + 1] + Dk[5] * pk[3 * c + 2];
       }
     }
-    // every thread has finished reading planes < k: stage slots of planes <= k-2 are free
+    // every thread is done with planes < k-1 (u, rc/gw) and with the p/D of plane k
     if (__syncthreads_or(bad)) {
       bad = true;
       break;
@@ -425,25 +482,26 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
     }
     const int j = k - 1;
     if (interior && j >= z0 && j < z1) {
-      const int ps = j % 3;
-      const S* RC = reinterpret_cast<const S*>(stage(j) + G::RC_OFF);
-      const S* GW = reinterpret_cast<const S*>(stage(j) + G::GW_OFF);
-      const int ri = (ty - 1) * TX + (tx - 1);
-      const float rcj = Store<S>::sh(RC + ri);
+      const int ps = (qs + 2) % 3;  // slot of plane j
+      const unsigned char* R = smem + G::R_OFF + ((j - kb) % G::NR) * G::R_SLOT;
+      const SP* RC = reinterpret_cast<const SP*>(R) + ro;
+      const SP* GW = reinterpret_cast<const SP*>(R + G::RC_SLOT) + ro;
+      const SU* Uj = ubox(j) + uo;
+      const Stencil3 az = adj_coef(j, nz, bdry, ihz);
+      const float rcj = Store<SP>::sh(RC);
       float gj[3], uj[3], div[3], un[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        gj[c] = Store<S>::sh(GW + c * TY * TX + ri);
-        uj[c] = uval(j, c, uy, ux);
-        const float ax = adj_axis(sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1], gx, nx, bdry);
-        const float ay = adj_axis(sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx], gy, ny, bdry);
-        const float az = adj_axis(qzmm[c], qzm[c], qzc[c], j, nz, bdry);
-        div[c] = (ax * ihx + ay * ihy) + az * ihz;
+        gj[c] = Store<SP>::sh(GW + c * TY * TX);
+        uj[c] = Store<SU>::sh(Uj + c * UYB * UXB);
+        const float dx = apply3(ax, sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1]);
+        const float dy = apply3(ay, sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx]);
+        div[c] = (dx + dy) + apply3(az, qzmm[c], qzm[c], qzc[c]);
       }
       primal_voxel(uj, div, a.tau, a.factor, rcj, gj, un);
-      const long long o = j * plane + col;
+      SU* dst = u_dst + j * plane + col;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) Store<S>::st(u_dst + c * cs + o, un[c]);
+      for (int c = 0; c < 3; ++c) Store<SU>::st(dst + c * cs, un[c]);
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -455,7 +513,10 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
     if (tid == 0) {
       atomicOr(status, SVS_DEV_TIMEOUT);
       // wait (bounded) for the copies this CTA still has in flight before it exits
-      for (int q = pl; q <= issued; ++q) mbar_wait(bars + (q - pl) % NSTG, (uint32_t)(((q - pl) / NSTG) & 1));
+      for (int q = max(waited + 1, pl); q <= issued; ++q) {
+        const int r = q - pl;
+        mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1));
+      }
     }
     return;
   }
@@ -463,24 +524,25 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
     const int j = nz - 1;
     if (interior && j >= z0) {
       const int ps = j % 3;
-      const S* RC = reinterpret_cast<const S*>(stage(j) + G::RC_OFF);
-      const S* GW = reinterpret_cast<const S*>(stage(j) + G::GW_OFF);
-      const int ri = (ty - 1) * TX + (tx - 1);
-      const float rcj = Store<S>::sh(RC + ri);
+      const unsigned char* R = smem + G::R_OFF + ((j - kb) % G::NR) * G::R_SLOT;
+      const SP* RC = reinterpret_cast<const SP*>(R) + ro;
+      const SP* GW = reinterpret_cast<const SP*>(R + G::RC_SLOT) + ro;
+      const SU* Uj = ubox(j) + uo;
+      const Stencil3 az = adj_coef(j, nz, bdry, ihz);
+      const float rcj = Store<SP>::sh(RC);
       float gj[3], uj[3], div[3], un[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        gj[c] = Store<S>::sh(GW + c * TY * TX + ri);
-        uj[c] = uval(j, c, uy, ux);
-        const float ax = adj_axis(sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1], gx, nx, bdry);
-        const float ay = adj_axis(sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx], gy, ny, bdry);
-        const float az = adj_axis(qzmm[c], qzm[c], 0.f, j, nz, bdry);
-        div[c] = (ax * ihx + ay * ihy) + az * ihz;
+        gj[c] = Store<SP>::sh(GW + c * TY * TX);
+        uj[c] = Store<SU>::sh(Uj + c * UYB * UXB);
+        const float dx = apply3(ax, sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1]);
+        const float dy = apply3(ay, sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx]);
+        div[c] = (dx + dy) + apply3(az, qzmm[c], qzm[c], 0.f);
       }
       primal_voxel(uj, div, a.tau, a.factor, rcj, gj, un);
-      const long long o = j * plane + col;
+      SU* dst = u_dst + j * plane + col;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) Store<S>::st(u_dst + c * cs + o, un[c]);
+      for (int c = 0; c < 3; ++c) Store<SU>::st(dst + c * cs, un[c]);
     }
   }
 }

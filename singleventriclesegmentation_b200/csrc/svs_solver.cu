@@ -36,9 +36,9 @@ namespace {
 
 // Iterate-kernel variants compiled into the library (id 1..N; 0 = automatic).
 struct TileShape {
-  int tx, ty, nstg;  // nstg = 0: plain-load form; > 0: TMA form with that many stages
+  int tx, ty, dist;  // dist = 0: plain-load form; > 0: TMA form with that prefetch distance
 };
-constexpr TileShape kTileShapes[] = {{32, 8, 5}, {32, 8, 4}, {64, 4, 4}, {16, 16, 4}, {32, 16, 4},
+constexpr TileShape kTileShapes[] = {{32, 8, 2}, {32, 8, 3}, {64, 4, 2}, {16, 16, 2}, {32, 16, 2},
                                      {32, 8, 0}, {32, 4, 0}, {16, 16, 0}};
 constexpr int kNumTileShapes = sizeof(kTileShapes) / sizeof(kTileShapes[0]);
 
@@ -106,7 +106,7 @@ __global__ void restrict_kernel(const Desc* __restrict__ fine, const Desc* __res
 // anisotropic tensor from s, n, t1 (anisotropicDifferentialOps.cu:89-141) packed as the
 // symmetric matrix s n n^T + t1 t1^T (d00 d01 d02 d11 d12 d22), and (first level only) zero u, p.
 // Without anisotropy D is the identity (tvl13d.py:218-219, 231-232 skip the operator).
-template <typename S>
+template <typename SU, typename SP>
 __global__ void prepare_kernel(const Desc* __restrict__ descs, int use_aniso, float alpha,
                                float beta, int bdry, int zero_state, int src) {
   const Desc d = descs[blockIdx.y];
@@ -142,14 +142,14 @@ __global__ void prepare_kernel(const Desc* __restrict__ descs, int use_aniso, fl
     }
   }
   const long long o = pidx(d, z, y, x);
-  S* Dp = reinterpret_cast<S*>(d.D);
+  SP* Dp = reinterpret_cast<SP*>(d.D);
 #pragma unroll
-  for (int i = 0; i < 6; ++i) Store<S>::st(Dp + i * d.cs + o, D[i]);
+  for (int i = 0; i < 6; ++i) Store<SP>::st(Dp + i * d.cs + o, D[i]);
   if (zero_state) {
-    S* u = reinterpret_cast<S*>(d.u[src]);
-    S* p = reinterpret_cast<S*>(d.p[src]);
-    for (int i = 0; i < 3; ++i) Store<S>::st(u + i * d.cs + o, 0.f);
-    for (int i = 0; i < 9; ++i) Store<S>::st(p + i * d.cs + o, 0.f);
+    SU* u = reinterpret_cast<SU*>(d.u[src]);
+    SP* p = reinterpret_cast<SP*>(d.p[src]);
+    for (int i = 0; i < 3; ++i) Store<SU>::st(u + i * d.cs + o, 0.f);
+    for (int i = 0; i < 9; ++i) Store<SP>::st(p + i * d.cs + o, 0.f);
   }
 }
 
@@ -194,15 +194,15 @@ __device__ __forceinline__ void sample_cubic4(const float* __restrict__ I, const
 
 // Per-warp linearisation, tvl13d.py:196-201: I1w = I1(x+u), gw = (grad I1)(x+u),
 // rho_c = I1w - u.gw - I0.
-template <typename S>
+template <typename SU, typename SP>
 __global__ void linearise_kernel(const Desc* __restrict__ descs, int src, int interp, int bdry) {
   const Desc d = descs[blockIdx.y];
   const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (v >= d.n) return;
   const int x = (int)(v % d.nx), y = (int)((v / d.nx) % d.ny), z = (int)(v / ((int64_t)d.nx * d.ny));
   const long long o = pidx(d, z, y, x);
-  const S* u = reinterpret_cast<const S*>(d.u[src]);
-  const float u0 = Store<S>::ld(u + o), u1 = Store<S>::ld(u + d.cs + o), u2 = Store<S>::ld(u + 2 * d.cs + o);
+  const SU* u = reinterpret_cast<const SU*>(d.u[src]);
+  const float u0 = Store<SU>::ld(u + o), u1 = Store<SU>::ld(u + d.cs + o), u2 = Store<SU>::ld(u + 2 * d.cs + o);
   const float cx = (float)x * d.hx + u0;
   const float cy = (float)y * d.hy + u1;
   const float cz = (float)z * d.hz + u2;
@@ -217,16 +217,16 @@ __global__ void linearise_kernel(const Desc* __restrict__ descs, int src, int in
   }
   const float dot = u0 * s[1] + u1 * s[2] + u2 * s[3];
   const float rc = s[0] - dot - d.I0[v];
-  S* gw = reinterpret_cast<S*>(d.gw);
-  Store<S>::st(reinterpret_cast<S*>(d.rc) + o, rc);
-  Store<S>::st(gw + o, s[1]);
-  Store<S>::st(gw + d.cs + o, s[2]);
-  Store<S>::st(gw + 2 * d.cs + o, s[3]);
+  SP* gw = reinterpret_cast<SP*>(d.gw);
+  Store<SP>::st(reinterpret_cast<SP*>(d.rc) + o, rc);
+  Store<SP>::st(gw + o, s[1]);
+  Store<SP>::st(gw + d.cs + o, s[2]);
+  Store<SP>::st(gw + 2 * d.cs + o, s[3]);
 }
 
 // Coarse -> fine transfer of u (scaled by L_f/L_c per axis, tvl13d.py:151-153) and p
 // (tvl13d.py:158), prolongationOps.cu:561-625; writes the fine level's buffer 0.
-template <typename S>
+template <typename SU, typename SP>
 __global__ void prolong_kernel(const Desc* __restrict__ coarse, const Desc* __restrict__ fine,
                                int src, int interp, int bdry) {
   const Desc c = coarse[blockIdx.y], f = fine[blockIdx.y];
@@ -240,10 +240,10 @@ __global__ void prolong_kernel(const Desc* __restrict__ coarse, const Desc* __re
   const float kx = (float)((double)f.lx / (double)c.lx);
   const float ky = (float)((double)f.ly / (double)c.ly);
   const float kz = (float)((double)f.lz / (double)c.lz);
-  const S* uc = reinterpret_cast<const S*>(c.u[src]);
-  const S* pc = reinterpret_cast<const S*>(c.p[src]);
-  S* uf = reinterpret_cast<S*>(f.u[0]);
-  S* pf = reinterpret_cast<S*>(f.p[0]);
+  const SU* uc = reinterpret_cast<const SU*>(c.u[src]);
+  const SP* pc = reinterpret_cast<const SP*>(c.p[src]);
+  SU* uf = reinterpret_cast<SU*>(f.u[0]);
+  SP* pf = reinterpret_cast<SP*>(f.p[0]);
   const long long of = pidx(f, z, y, x);
   int ix, iy, iz;
   float wx, wy, wz;
@@ -251,8 +251,12 @@ __global__ void prolong_kernel(const Desc* __restrict__ coarse, const Desc* __re
   split_coord(cy, c.hy, iy, wy);
   split_coord(cz, c.hz, iz, wz);
   for (int comp = 0; comp < 12; ++comp) {
-    const S* F = comp < 3 ? uc + comp * c.cs : pc + (comp - 3) * c.cs;
-    auto at = [&](int zz, int yy, int xx) { return Store<S>::ld(F + pidx(c, zz, yy, xx)); };
+    const SU* FU = uc + comp * c.cs;
+    const SP* FP = pc + (comp - 3) * c.cs;
+    auto at = [&](int zz, int yy, int xx) {
+      const long long o = pidx(c, zz, yy, xx);
+      return comp < 3 ? Store<SU>::ld(FU + o) : Store<SP>::ld(FP + o);
+    };
     float val;
     if (interp == SVS_INTERPOLATE_CUBIC_HERMITESPLINE) {
       float bz[4];
@@ -285,15 +289,15 @@ __global__ void prolong_kernel(const Desc* __restrict__ coarse, const Desc* __re
     }
     if (comp < 3) {
       const float k = comp == 0 ? kx : (comp == 1 ? ky : kz);
-      Store<S>::st(uf + comp * f.cs + of, val * k);
+      Store<SU>::st(uf + comp * f.cs + of, val * k);
     } else {
-      Store<S>::st(pf + (comp - 3) * f.cs + of, val);
+      Store<SP>::st(pf + (comp - 3) * f.cs + of, val);
     }
   }
 }
 
 // Level 0 planar state -> the caller's AoS layouts: u [Z,Y,X,3], p [Z,Y,X,3,3].
-template <typename S>
+template <typename SU, typename SP>
 __global__ void finalize_kernel(const Desc* __restrict__ descs, int src, float* const* __restrict__ u_out,
                                 float* const* __restrict__ p_out) {
   const Desc d = descs[blockIdx.y];
@@ -301,19 +305,19 @@ __global__ void finalize_kernel(const Desc* __restrict__ descs, int src, float* 
   if (v >= d.n) return;
   const int x = (int)(v % d.nx), y = (int)((v / d.nx) % d.ny), z = (int)(v / ((int64_t)d.nx * d.ny));
   const long long o = pidx(d, z, y, x);
-  const S* u = reinterpret_cast<const S*>(d.u[src]);
+  const SU* u = reinterpret_cast<const SU*>(d.u[src]);
   float* uo = u_out[blockIdx.y];
-  for (int c = 0; c < 3; ++c) uo[3 * v + c] = Store<S>::ld(u + c * d.cs + o);
+  for (int c = 0; c < 3; ++c) uo[3 * v + c] = Store<SU>::ld(u + c * d.cs + o);
   float* po = p_out[blockIdx.y];
   if (po) {
-    const S* p = reinterpret_cast<const S*>(d.p[src]);
-    for (int c = 0; c < 9; ++c) po[9 * v + c] = Store<S>::ld(p + c * d.cs + o);
+    const SP* p = reinterpret_cast<const SP*>(d.p[src]);
+    for (int c = 0; c < 9; ++c) po[9 * v + c] = Store<SP>::ld(p + c * d.cs + o);
   }
 }
 
 // Optional warm start (num_scales == 1 only: otherwise the reference overwrites u and p,
 // tvl13d.py:150, 158): AoS caller fields -> level-0 planar buffer 0.
-template <typename S>
+template <typename SU, typename SP>
 __global__ void warm_start_kernel(const Desc* __restrict__ descs, const float* const* __restrict__ u_in,
                                   const float* const* __restrict__ p_in) {
   const Desc d = descs[blockIdx.y];
@@ -323,10 +327,10 @@ __global__ void warm_start_kernel(const Desc* __restrict__ descs, const float* c
   const long long o = pidx(d, z, y, x);
   const float* ui = u_in[blockIdx.y];
   const float* pi = p_in[blockIdx.y];
-  S* u = reinterpret_cast<S*>(d.u[0]);
-  S* p = reinterpret_cast<S*>(d.p[0]);
-  for (int c = 0; c < 3; ++c) Store<S>::st(u + c * d.cs + o, ui ? ui[3 * v + c] : 0.f);
-  for (int c = 0; c < 9; ++c) Store<S>::st(p + c * d.cs + o, pi ? pi[9 * v + c] : 0.f);
+  SU* u = reinterpret_cast<SU*>(d.u[0]);
+  SP* p = reinterpret_cast<SP*>(d.p[0]);
+  for (int c = 0; c < 3; ++c) Store<SU>::st(u + c * d.cs + o, ui ? ui[3 * v + c] : 0.f);
+  for (int c = 0; c < 9; ++c) Store<SP>::st(p + c * d.cs + o, pi ? pi[9 * v + c] : 0.f);
 }
 
 }  // namespace
@@ -375,7 +379,14 @@ struct svs_plan {
 namespace svs {
 namespace {
 
-size_t storage_bytes(int storage) { return storage == SVS_STORAGE_F32 ? 4 : 2; }
+// Storage of the flow (u) and of the other iteration fields (p, D, rc, gw).
+size_t flow_bytes(int storage) { return (storage == SVS_STORAGE_BF16 || storage == SVS_STORAGE_F16) ? 2 : 4; }
+size_t field_bytes(int storage) { return storage == SVS_STORAGE_F32 ? 4 : 2; }
+CUtensorMapDataType map_type(int bytes, bool bf16) {
+  return bytes == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                    : (bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16);
+}
+bool is_bf16(int storage) { return storage == SVS_STORAGE_BF16 || storage == SVS_STORAGE_BF16_FLOW32; }
 
 // ---------------------------------------------------------------------- TMA tensor maps
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -392,13 +403,12 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // A 4D map (x, y, z, component) over one pitched planar field, box {bx, by, 1, bc}.
-bool encode_field(CUtensorMap* m, int storage, const void* base, const Desc& d, int comps, int bx, int by) {
+bool encode_field(CUtensorMap* m, int es_bytes, bool bf16, const void* base, const Desc& d, int comps, int bx,
+                  int by) {
   auto fn = encode_fn();
   if (!fn) return false;
-  const CUtensorMapDataType dt = storage == SVS_STORAGE_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
-                                 : storage == SVS_STORAGE_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
-                                                               : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
-  const cuuint64_t es = storage_bytes(storage);
+  const CUtensorMapDataType dt = map_type(es_bytes, bf16);
+  const cuuint64_t es = (cuuint64_t)es_bytes;
   cuuint64_t gdim[4] = {(cuuint64_t)d.nx, (cuuint64_t)d.ny, (cuuint64_t)d.nz, (cuuint64_t)comps};
   cuuint64_t gstride[3] = {(cuuint64_t)d.pitch * es, (cuuint64_t)d.pitch * d.ny * es, (cuuint64_t)d.cs * es};
   cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1u, (cuuint32_t)comps};
@@ -409,60 +419,61 @@ bool encode_field(CUtensorMap* m, int storage, const void* base, const Desc& d, 
   return r == CUDA_SUCCESS;
 }
 
-template <typename S, int TX, int TY, int NSTG>
+template <typename SU, typename SP, int TX, int TY, int DIST>
 bool encode_maps(svs_plan& P, std::vector<TMaps>& maps, int level) {
-  using G = TmaGeom<S, TX, TY, NSTG>;
+  using G = TmaGeom<SU, SP, TX, TY, DIST>;
+  const bool bf = is_bf16(P.prm.storage);
   for (int i = 0; i < P.num_pairs; ++i) {
     const size_t k = (size_t)level * P.num_pairs + i;
     const Desc& d = P.h_descs[k];
     TMaps& m = maps[k];
-    const int st = P.prm.storage;
-    bool ok = encode_field(&m.u[0], st, d.u[0], d, 3, G::UXB, G::UYB) &&
-              encode_field(&m.u[1], st, d.u[1], d, 3, G::UXB, G::UYB) &&
-              encode_field(&m.p[0], st, d.p[0], d, 9, G::PXB, G::PYB) &&
-              encode_field(&m.p[1], st, d.p[1], d, 9, G::PXB, G::PYB) &&
-              encode_field(&m.D, st, d.D, d, 6, G::PXB, G::PYB) &&
-              encode_field(&m.rc, st, d.rc, d, 1, TX, TY) && encode_field(&m.gw, st, d.gw, d, 3, TX, TY);
+    bool ok = encode_field(&m.u[0], G::ESU, bf, d.u[0], d, 3, G::UXB, G::UYB) &&
+              encode_field(&m.u[1], G::ESU, bf, d.u[1], d, 3, G::UXB, G::UYB) &&
+              encode_field(&m.p[0], G::ESP, bf, d.p[0], d, 9, G::PXB, G::PYB) &&
+              encode_field(&m.p[1], G::ESP, bf, d.p[1], d, 9, G::PXB, G::PYB) &&
+              encode_field(&m.D, G::ESP, bf, d.D, d, 6, G::PXB, G::PYB) &&
+              encode_field(&m.rc, G::ESP, bf, d.rc, d, 1, TX, TY) &&
+              encode_field(&m.gw, G::ESP, bf, d.gw, d, 3, TX, TY);
     if (!ok) return false;
   }
   return true;
 }
 
-template <typename S, int TX, int TY, int NSTG>
+template <typename SU, typename SP, int TX, int TY, int DIST>
 bool tma_prepare(svs_plan& P, std::vector<TMaps>& maps, int level) {
-  using G = TmaGeom<S, TX, TY, NSTG>;
+  using G = TmaGeom<SU, SP, TX, TY, DIST>;
   if (G::SMEM > 227 * 1024) return false;
-  if (cudaFuncSetAttribute(iterate_tma_kernel<S, TX, TY, NSTG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute(iterate_tma_kernel<SU, SP, TX, TY, DIST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            G::SMEM) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return encode_maps<S, TX, TY, NSTG>(P, maps, level);
+  return encode_maps<SU, SP, TX, TY, DIST>(P, maps, level);
 }
 
 // Dispatch over the compiled variants. `op` 0: prepare (attributes + maps), 1: launch.
-template <typename S>
+template <typename SU, typename SP>
 bool iter_variant(svs_plan& P, std::vector<TMaps>* maps, int level, int tid, int op, const IterArgs* a,
                   cudaStream_t s) {
   const unsigned nt = (unsigned)P.h_tiles[level].size();
   const Tile* tl = P.d_tiles.empty() ? nullptr : P.d_tiles[level];
-#define SVS_TMA_CASE(ID, TX, TY, NS)                                                                  \
-  case ID:                                                                                            \
-    if (op == 0) return tma_prepare<S, TX, TY, NS>(P, *maps, level);                                   \
-    iterate_tma_kernel<S, TX, TY, NS><<<nt, (TX + 2) * (TY + 2), TmaGeom<S, TX, TY, NS>::SMEM, s>>>(  \
-        tl, P.d_descs, P.d_maps, *a, P.d_status);                                                     \
+#define SVS_TMA_CASE(ID, TX, TY, DS)                                                                      \
+  case ID:                                                                                                \
+    if (op == 0) return tma_prepare<SU, SP, TX, TY, DS>(P, *maps, level);                                \
+    iterate_tma_kernel<SU, SP, TX, TY, DS><<<nt, (TX + 2) * (TY + 2), TmaGeom<SU, SP, TX, TY, DS>::SMEM, s>>>( \
+        tl, P.d_descs, P.d_maps, *a, P.d_status);                                                         \
     return true;
 #define SVS_PLAIN_CASE(ID, TX, TY)                                                                   \
   case ID:                                                                                           \
     if (op == 0) return true;                                                                        \
-    iterate_kernel<S, TX, TY><<<nt, (TX + 2) * (TY + 2), 0, s>>>(tl, P.d_descs, *a);                 \
+    iterate_kernel<SU, SP, TX, TY><<<nt, (TX + 2) * (TY + 2), 0, s>>>(tl, P.d_descs, *a);            \
     return true;
   switch (tid) {
-    SVS_TMA_CASE(1, 32, 8, 5)
-    SVS_TMA_CASE(2, 32, 8, 4)
-    SVS_TMA_CASE(3, 64, 4, 4)
-    SVS_TMA_CASE(4, 16, 16, 4)
-    SVS_TMA_CASE(5, 32, 16, 4)
+    SVS_TMA_CASE(1, 32, 8, 2)
+    SVS_TMA_CASE(2, 32, 8, 3)
+    SVS_TMA_CASE(3, 64, 4, 2)
+    SVS_TMA_CASE(4, 16, 16, 2)
+    SVS_TMA_CASE(5, 32, 16, 2)
     SVS_PLAIN_CASE(6, 32, 8)
     SVS_PLAIN_CASE(7, 32, 4)
     SVS_PLAIN_CASE(8, 16, 16)
@@ -474,14 +485,21 @@ bool iter_variant(svs_plan& P, std::vector<TMaps>* maps, int level, int tid, int
 
 bool iter_dispatch(svs_plan& P, std::vector<TMaps>* maps, int level, int tid, int op, const IterArgs* a,
                    cudaStream_t s) {
-  if (P.prm.storage == SVS_STORAGE_BF16) return iter_variant<__nv_bfloat16>(P, maps, level, tid, op, a, s);
-  if (P.prm.storage == SVS_STORAGE_F16) return iter_variant<__half>(P, maps, level, tid, op, a, s);
-  return iter_variant<float>(P, maps, level, tid, op, a, s);
+  switch (P.prm.storage) {
+    case SVS_STORAGE_BF16: return iter_variant<__nv_bfloat16, __nv_bfloat16>(P, maps, level, tid, op, a, s);
+    case SVS_STORAGE_F16: return iter_variant<__half, __half>(P, maps, level, tid, op, a, s);
+    case SVS_STORAGE_BF16_FLOW32: return iter_variant<float, __nv_bfloat16>(P, maps, level, tid, op, a, s);
+    case SVS_STORAGE_F16_FLOW32: return iter_variant<float, __half>(P, maps, level, tid, op, a, s);
+    default: return iter_variant<float, float>(P, maps, level, tid, op, a, s);
+  }
 }
 
-// Automatic choice: the 5-stage 32x8 TMA pipeline for 4-byte storage, the 4-stage one (two CTAs
-// per SM) for 2-byte storage; the plain-load 32x8 form if TMA descriptors cannot be built.
-int auto_tile(const svs_plan& P) { return P.prm.storage == SVS_STORAGE_F32 ? 1 : 2; }
+// Automatic choice: the 32x8 TMA pipeline with prefetch distance 2 (two CTAs per SM); the
+// plain-load 32x8 form if TMA descriptors cannot be built.
+int auto_tile(const svs_plan& P) {
+  (void)P;
+  return 1;
+}
 
 void build_tiles(svs_plan& P, int level, int tid) {
   const TileShape ts = kTileShapes[tid - 1];
@@ -556,7 +574,7 @@ IterArgs iter_args(const svs_plan& P, int it, int cur) {
 
 // The whole batched solve as a sequence of launches on stream s. Returns the number of kernel
 // launches issued or -1 after a launch error.
-template <typename S>
+template <typename SU, typename SP>
 long long enqueue_solve(svs_plan& P, cudaStream_t s) {
   const svs_tvl1_params& q = P.prm;
   const int L = P.levels, np = P.num_pairs;
@@ -570,16 +588,16 @@ long long enqueue_solve(svs_plan& P, cudaStream_t s) {
     ++launches;
   }
   if (P.warm && L == 1) {
-    warm_start_kernel<S><<<grid(0), 256, 0, s>>>(D, P.d_uinit, P.d_pinit);
+    warm_start_kernel<SU, SP><<<grid(0), 256, 0, s>>>(D, P.d_uinit, P.d_pinit);
     ++launches;
   }
   int cur = 0;
   for (int l = L - 1; l >= 0; --l) {
     const int zero = (l == L - 1) && !(P.warm && L == 1);
-    prepare_kernel<S><<<grid(l), 256, 0, s>>>(D + (size_t)l * np, q.use_anisotropic_diff, q.alpha, q.beta, q.boundary, zero, cur);
+    prepare_kernel<SU, SP><<<grid(l), 256, 0, s>>>(D + (size_t)l * np, q.use_anisotropic_diff, q.alpha, q.beta, q.boundary, zero, cur);
     ++launches;
     for (int w = 0; w < q.max_warps; ++w) {
-      linearise_kernel<S><<<grid(l), 256, 0, s>>>(D + (size_t)l * np, cur, q.interpolation, q.boundary);
+      linearise_kernel<SU, SP><<<grid(l), 256, 0, s>>>(D + (size_t)l * np, cur, q.interpolation, q.boundary);
       ++launches;
       for (int it = 0; it < q.max_outer_iterations; ++it) {
         const IterArgs a = iter_args(P, it, cur);
@@ -589,13 +607,13 @@ long long enqueue_solve(svs_plan& P, cudaStream_t s) {
       }
     }
     if (l > 0) {
-      prolong_kernel<S><<<grid(l - 1), 256, 0, s>>>(D + (size_t)l * np, D + (size_t)(l - 1) * np, cur, q.interpolation, q.boundary);
+      prolong_kernel<SU, SP><<<grid(l - 1), 256, 0, s>>>(D + (size_t)l * np, D + (size_t)(l - 1) * np, cur, q.interpolation, q.boundary);
       ++launches;
       cur = 0;
     }
   }
   float** uo = q.median_kernel > 1 ? P.d_umed : P.d_uout;
-  finalize_kernel<S><<<grid(0), 256, 0, s>>>(D, cur, uo, P.d_pout);
+  finalize_kernel<SU, SP><<<grid(0), 256, 0, s>>>(D, cur, uo, P.d_pout);
   ++launches;
   if (cudaPeekAtLastError() != cudaSuccess) return -1;
   if (q.median_kernel > 1) {
@@ -609,9 +627,13 @@ long long enqueue_solve(svs_plan& P, cudaStream_t s) {
 }
 
 long long enqueue(svs_plan& P, cudaStream_t s) {
-  if (P.prm.storage == SVS_STORAGE_BF16) return enqueue_solve<__nv_bfloat16>(P, s);
-  if (P.prm.storage == SVS_STORAGE_F16) return enqueue_solve<__half>(P, s);
-  return enqueue_solve<float>(P, s);
+  switch (P.prm.storage) {
+    case SVS_STORAGE_BF16: return enqueue_solve<__nv_bfloat16, __nv_bfloat16>(P, s);
+    case SVS_STORAGE_F16: return enqueue_solve<__half, __half>(P, s);
+    case SVS_STORAGE_BF16_FLOW32: return enqueue_solve<float, __nv_bfloat16>(P, s);
+    case SVS_STORAGE_F16_FLOW32: return enqueue_solve<float, __half>(P, s);
+    default: return enqueue_solve<float, float>(P, s);
+  }
 }
 
 template <typename T> T* carve(char*& cur, size_t count) {
@@ -639,7 +661,7 @@ svs_status svs_tvl1_plan_create(const svs_tvl1_params* prm, int num_pairs, const
               "svs_tvl1_plan_create: primaldual_algorithm_type must be 1 or 2");
   SVS_REQUIRE(prm->boundary >= 0 && prm->boundary <= 2, "svs_tvl1_plan_create: bad boundary type");
   SVS_REQUIRE(prm->interpolation >= 0 && prm->interpolation <= 2, "svs_tvl1_plan_create: bad interpolation type");
-  SVS_REQUIRE(prm->storage >= 0 && prm->storage <= 2, "svs_tvl1_plan_create: bad storage type");
+  SVS_REQUIRE(prm->storage >= 0 && prm->storage <= 4, "svs_tvl1_plan_create: bad storage type");
   SVS_REQUIRE(prm->weight_tv >= 0.f, "svs_tvl1_plan_create: weight_tv must be >= 0");
   SVS_REQUIRE(prm->median_kernel == 0 || prm->median_kernel == 1 || prm->median_kernel == 3 ||
                   prm->median_kernel == 5 || prm->median_kernel == 7,
@@ -652,7 +674,7 @@ svs_status svs_tvl1_plan_create(const svs_tvl1_params* prm, int num_pairs, const
   // mesh sizes per level (tvl13d.py:91-99, ceil halving) and spacings (coreDefines.h:72-75)
   P->h_descs.resize((size_t)P->levels * num_pairs);
   size_t bytes = 0;
-  const size_t sb = storage_bytes(prm->storage);
+  const size_t ub = flow_bytes(prm->storage), sb = field_bytes(prm->storage);
   auto al = [](size_t b) { return (b + 255) / 256 * 256; };
   for (int i = 0; i < num_pairs; ++i) {
     int nz = dims[3 * i], ny = dims[3 * i + 1], nx = dims[3 * i + 2];
@@ -675,7 +697,8 @@ svs_status svs_tvl1_plan_create(const svs_tvl1_params* prm, int num_pairs, const
       const size_t n = (size_t)d.n, cs = (size_t)d.cs;
       bytes += 2 * al(n * 4) + al(3 * n * 4);                       // I0, I1, g1
       bytes += al(6 * cs * sb) + al(cs * sb) + al(3 * cs * sb);      // D, rc, gw
-      bytes += 2 * al(3 * cs * sb) + 2 * al(9 * cs * sb);            // u[2], p[2]
+      bytes += 2 * al(3 * cs * ub) + 2 * al(9 * cs * sb);            // u[2], p[2]
+      if (9 * cs >= (size_t)1 << 31) { delete P; return fail(SVS_ERR_INVALID_ARG, "svs_tvl1_plan_create: volume too large for 32-bit field offsets"); }
       if (l == 0) bytes += 2 * al(n * 4) + 2 * al(3 * n * 4) + al(9 * n * 4);  // raw x2, uout, umed, pout
     }
   }
@@ -699,8 +722,8 @@ svs_status svs_tvl1_plan_create(const svs_tvl1_params* prm, int num_pairs, const
       d.D = carve<char>(cur, 6 * cs * sb);
       d.rc = carve<char>(cur, cs * sb);
       d.gw = carve<char>(cur, 3 * cs * sb);
-      d.u[0] = carve<char>(cur, 3 * cs * sb);
-      d.u[1] = carve<char>(cur, 3 * cs * sb);
+      d.u[0] = carve<char>(cur, 3 * cs * ub);
+      d.u[1] = carve<char>(cur, 3 * cs * ub);
       d.p[0] = carve<char>(cur, 9 * cs * sb);
       d.p[1] = carve<char>(cur, 9 * cs * sb);
       if (l == 0) {
