@@ -143,6 +143,11 @@ iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, I
   const bool ring_on = tid < NRING && rgx >= 0 && rgx < nx && rgy >= 0 && rgy < ny;
   const int rcol = rgy * Dg.pitch + rgx;
 
+  // Cells of out-of-domain columns are never written but are multiplied by zero stencil
+  // coefficients at the domain faces: they must hold zeros, not stale bits (0 * NaN = NaN).
+  for (int i = tid; i < 2 * 3 * UY * UX; i += blockDim.x) (&su[0][0][0][0])[i] = 0.f;
+  for (int i = tid; i < 2 * 6 * PY * PX; i += blockDim.x) (&sq[0][0][0][0])[i] = 0.f;
+  __syncthreads();
   const int kb = max(z0 - 1, 0), ke = min(z1, nz - 1);
   float um[3] = {0.f, 0.f, 0.f}, uc[3] = {0.f, 0.f, 0.f}, up[3] = {0.f, 0.f, 0.f};
   if (in_dom) {
@@ -412,6 +417,9 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
     return reinterpret_cast<const SU*>(smem + G::U_OFF + ((q - pl) % G::NU) * G::U_SLOT);
   };
 
+  // Published rows of out-of-domain columns are never written but are multiplied by zero
+  // stencil coefficients at the domain faces: they must hold zeros (0 * NaN = NaN).
+  for (int i = tid; i < 3 * 6 * PY * PX; i += blockDim.x) (&sq[0][0][0][0])[i] = 0.f;
   if (tid == 0) {
     for (int s = 0; s < G::NB; ++s) mbar_init(bars + s, 1);
     mbar_fence_init();
