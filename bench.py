@@ -137,7 +137,12 @@ def oracle_sample(threads: int):
     o.build()
     o.set_threads(threads)
     I0, I1, _ = synthetic.frame_pair(SHAPE, seed=0)
-    k = 24
+    # calibrate the iteration count so that the sample is about 10 s of host work
+    probe = 8
+    t0 = time.perf_counter()
+    o.tvl1_compute(I0, I1, o.SolverParams(max_warps=1, max_outer_iterations=probe), dtype=np.float32)
+    per_it = (time.perf_counter() - t0) / probe
+    k = int(min(4500, max(probe, 10.0 / max(per_it, 1e-6))))
     P = o.SolverParams(max_warps=1, max_outer_iterations=k)
     t0 = time.perf_counter()
     o.tvl1_compute(I0, I1, P, dtype=np.float32)

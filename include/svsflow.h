@@ -188,6 +188,8 @@ size_t svs_tvl1_plan_device_bytes(const svs_plan* plan);
  * unknown id. Variants 1-5 are TMA pipelines (tile x prefetch distance: 32x8/2, 32x8/3, 64x4/2, 16x16/2, 32x16/2),
  * 6-8 plain-load forms (32x8, 32x4, 16x16). Used by the autotuner. */
 svs_status svs_tvl1_plan_set_tile(svs_plan* plan, int tile_id);
+/* Same for one pyramid level only (0 = fall back to the plan-wide choice). */
+svs_status svs_tvl1_plan_set_level_tile(svs_plan* plan, int level, int tile_id);
 int svs_tvl1_num_tiles(void);
 
 /* Solve every pair of the plan (pairs[i] must match dims[i] of the plan). */
@@ -196,8 +198,8 @@ svs_status svs_tvl1_solve_batch(svs_plan* plan, const svs_pair_desc* pairs_host,
 
 /* Benchmark hook: launch `count` iterate kernels (the fused primal-dual iteration) of pyramid
  * level `level` on the plan's current state, alternating its ping-pong buffers. Used to time the
- * dominant kernel on live data; it overwrites the plan's iteration state (results already copied
- * out by svs_tvl1_solve_batch are unaffected). Requires one earlier solve. */
+ * dominant kernel on live data and by the autotuner; it overwrites the plan's iteration state
+ * (results already copied out by svs_tvl1_solve_batch are unaffected). */
 svs_status svs_tvl1_bench_iterations(svs_plan* plan, int level, int count, svs_stream_t stream);
 /* Number of kernel nodes in the plan's captured solve graph (0 before the first solve). */
 uint64_t svs_tvl1_plan_graph_kernels(const svs_plan* plan);

@@ -69,6 +69,7 @@ _SIGS = {
     "svs_tvl1_plan_destroy": (c_int, [c_void_p]),
     "svs_tvl1_plan_device_bytes": (c_size_t, [c_void_p]),
     "svs_tvl1_plan_set_tile": (c_int, [c_void_p, c_int]),
+    "svs_tvl1_plan_set_level_tile": (c_int, [c_void_p, c_int, c_int]),
     "svs_tvl1_num_tiles": (c_int, []),
     "svs_tvl1_solve_batch": (c_int, [c_void_p, ctypes.POINTER(PairDesc), c_int, c_void_p]),
     "svs_tvl1_bench_iterations": (c_int, [c_void_p, c_int, c_int, c_void_p]),

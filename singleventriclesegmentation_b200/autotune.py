@@ -1,0 +1,93 @@
+"""Autotuner for the fused iterate kernel: picks, per pyramid level of a plan, the kernel variant
+(TMA pipeline or plain-load form, tile shape, prefetch distance) with the shortest measured time
+on the plan's own state, and caches the choice on disk.
+
+The variants are listed in include/svsflow.h (svs_tvl1_plan_set_tile). A level's "size class" is
+the multiset of its volume sizes; the cache key is (GPU name, storage, level sizes).
+"""
+from __future__ import annotations
+
+import json
+import os
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import torch
+
+from . import _lib
+from .tvl13d import SolverPlan
+
+CACHE = os.environ.get("SVS_AUTOTUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "svsflow", "autotune.json"))
+
+
+def _level_dims(dims: Sequence[Tuple[int, int, int]], levels: int) -> List[List[Tuple[int, int, int]]]:
+    out = []
+    cur = [tuple(d) for d in dims]
+    for _ in range(levels):
+        out.append(sorted(cur))
+        cur = [tuple((v + 1) // 2 for v in d) for d in cur]
+    return out
+
+
+def _key(device, storage: str, level_dims) -> str:
+    name = torch.cuda.get_device_name(device).replace(" ", "_")
+    sig = ";".join("x".join(map(str, d)) for d in level_dims)
+    return f"{name}|{storage}|{sig}"
+
+
+def _load() -> Dict[str, int]:
+    try:
+        with open(CACHE) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(db: Dict[str, int]) -> None:
+    try:
+        os.makedirs(os.path.dirname(CACHE), exist_ok=True)
+        tmp = CACHE + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(db, f, indent=1, sort_keys=True)
+        os.replace(tmp, CACHE)
+    except OSError:
+        pass
+
+
+def time_variant(plan: SolverPlan, level: int, tile: int, iters: int = 6) -> Optional[float]:
+    """Mean milliseconds per launch of `tile` at `level`, or None if the variant does not fit."""
+    plan.set_level_tile(level, tile)
+    try:
+        plan.bench_iterations(level, 2)
+    except _lib.SVSError as e:
+        if e.status == 5:  # shared memory or descriptor limits
+            return None
+        raise
+    torch.cuda.synchronize(plan.device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    plan.bench_iterations(level, iters)
+    e1.record()
+    torch.cuda.synchronize(plan.device)
+    return e0.elapsed_time(e1) / iters
+
+
+def tune(plan: SolverPlan, storage: str, levels: int, candidates: Optional[Sequence[int]] = None,
+         use_cache: bool = True, iters: int = 6) -> List[int]:
+    """Choose and set the fastest variant per level; returns the chosen ids (level 0 first)."""
+    candidates = list(candidates or range(1, int(_lib.lib().svs_tvl1_num_tiles()) + 1))
+    db = _load() if use_cache else {}
+    chosen = []
+    lds = _level_dims(plan.dims, levels)
+    for level in range(levels):
+        key = _key(plan.device, storage, [lds[level]])
+        best = db.get(key)
+        if best is None:
+            timings = {t: time_variant(plan, level, t, iters) for t in candidates}
+            timings = {t: v for t, v in timings.items() if v is not None}
+            best = min(timings, key=timings.get)
+            db[key] = best
+        plan.set_level_tile(level, best)
+        chosen.append(best)
+    if use_cache:
+        _store(db)
+    return chosen

@@ -350,8 +350,10 @@ struct svs_plan {
   std::vector<std::vector<svs::Tile>> h_tiles;  // per level
   std::vector<svs::Tile*> d_tiles;
   std::vector<int> level_tile;             // tile id used per level
-  int tile_id = 0;                         // requested (0 = automatic)
+  std::vector<int> level_tile_req;         // per-level request (0 = use tile_id)
+  int tile_id = 0;                         // requested for all levels (0 = automatic)
   int tiles_built_for = -1;
+  int tile_epoch = 0;                      // bumped on every tile request change
   void* arena = nullptr;
   size_t arena_bytes = 0;
   int* d_status = nullptr;                 // device error bits (SVS_DEV_*)
@@ -533,10 +535,11 @@ svs_status setup_tiles(svs_plan& P) {
   std::vector<TMaps> maps((size_t)P.levels * P.num_pairs);
   std::memset(maps.data(), 0, maps.size() * sizeof(TMaps));
   for (int l = 0; l < P.levels; ++l) {
-    int tid = want > 0 ? want : auto_tile(P);
+    const int req = (l < (int)P.level_tile_req.size() && P.level_tile_req[l] > 0) ? P.level_tile_req[l] : want;
+    int tid = req > 0 ? req : auto_tile(P);
     build_tiles(P, l, tid);
     if (!iter_dispatch(P, &maps, l, tid, 0, nullptr, nullptr)) {
-      if (want > 0) return fail(SVS_ERR_UNSUPPORTED, "tile variant not usable for this plan (shared memory or TMA descriptor limits)");
+      if (req > 0) return fail(SVS_ERR_UNSUPPORTED, "tile variant not usable for this plan (shared memory or TMA descriptor limits)");
       tid = 6;  // plain-load 32x8
       build_tiles(P, l, tid);
     }
@@ -813,6 +816,17 @@ svs_status svs_tvl1_plan_set_tile(svs_plan* P, int tile_id) {
   SVS_REQUIRE(P, "svs_tvl1_plan_set_tile: null plan");
   SVS_REQUIRE(tile_id >= 0 && tile_id <= kNumTileShapes, "svs_tvl1_plan_set_tile: unknown tile id");
   P->tile_id = tile_id;
+  ++P->tile_epoch;
+  return SVS_OK;
+}
+
+svs_status svs_tvl1_plan_set_level_tile(svs_plan* P, int level, int tile_id) {
+  SVS_REQUIRE(P, "svs_tvl1_plan_set_level_tile: null plan");
+  SVS_REQUIRE(level >= 0 && level < P->levels, "svs_tvl1_plan_set_level_tile: bad level");
+  SVS_REQUIRE(tile_id >= 0 && tile_id <= kNumTileShapes, "svs_tvl1_plan_set_level_tile: unknown tile id");
+  if ((int)P->level_tile_req.size() < P->levels) P->level_tile_req.resize(P->levels, 0);
+  P->level_tile_req[level] = tile_id;
+  ++P->tile_epoch;
   return SVS_OK;
 }
 
@@ -853,12 +867,12 @@ svs_status svs_tvl1_solve_batch(svs_plan* P, const svs_pair_desc* pairs, int num
     P->want_p = want_p;
   }
   P->warm = warm;
-  if (P->tiles_built_for != P->tile_id) {
+  if (P->tiles_built_for != P->tile_epoch) {
     st = setup_tiles(*P);
     if (st) return st;
-    P->tiles_built_for = P->tile_id;
+    P->tiles_built_for = P->tile_epoch;
   }
-  if (!P->exec || P->graph_tile != P->tile_id || P->graph_warm != warm || P->graph_want_p != want_p) {
+  if (!P->exec || P->graph_tile != P->tile_epoch || P->graph_warm != warm || P->graph_want_p != want_p) {
     if (P->exec) { cudaGraphExecDestroy(P->exec); P->exec = nullptr; }
     cudaGraph_t g = nullptr;
     st = check_cuda(cudaStreamBeginCapture(P->cap_stream, cudaStreamCaptureModeThreadLocal), "solve: capture");
@@ -872,7 +886,7 @@ svs_status svs_tvl1_solve_batch(svs_plan* P, const svs_pair_desc* pairs, int num
     cudaGraphDestroy(g);
     if (st) return st;
     P->graph_kernels = (uint64_t)nl;
-    P->graph_tile = P->tile_id;
+    P->graph_tile = P->tile_epoch;
     P->graph_warm = warm;
     P->graph_want_p = want_p;
   }
@@ -892,7 +906,11 @@ svs_status svs_tvl1_bench_iterations(svs_plan* P, int level, int count, svs_stre
   SVS_REQUIRE(P, "svs_tvl1_bench_iterations: null plan");
   SVS_REQUIRE(level >= 0 && level < P->levels, "svs_tvl1_bench_iterations: bad level");
   SVS_REQUIRE(count >= 0, "svs_tvl1_bench_iterations: bad count");
-  SVS_REQUIRE(P->tiles_built_for == P->tile_id, "svs_tvl1_bench_iterations: run a solve first");
+  if (P->tiles_built_for != P->tile_epoch) {
+    const svs_status st = setup_tiles(*P);
+    if (st) return st;
+    P->tiles_built_for = P->tile_epoch;
+  }
   int cur = 0;
   for (int i = 0; i < count; ++i) {
     const int it = P->prm.max_outer_iterations > 0 ? i % P->prm.max_outer_iterations : 0;

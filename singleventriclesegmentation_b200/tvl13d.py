@@ -42,6 +42,9 @@ class SolverPlan:
     def set_tile(self, tile_id: int) -> None:
         check(_lib.lib().svs_tvl1_plan_set_tile(self._h, int(tile_id)))
 
+    def set_level_tile(self, level: int, tile_id: int) -> None:
+        check(_lib.lib().svs_tvl1_plan_set_level_tile(self._h, int(level), int(tile_id)))
+
     def solve(self, I0s, I1s, u_outs, p_outs=None, u_inits=None, p_inits=None, stream=None):
         n = len(self.dims)
         descs = (PairDesc * n)()
