@@ -210,6 +210,24 @@ int svs_tvl1_plan_level_tile(const svs_plan* plan, int level);
  * solve are invalid), SVS_OK otherwise. */
 svs_status svs_tvl1_plan_check(svs_plan* plan);
 
+/* Allocation-free solve of ONE frame pair, for callers that cannot call cudaMalloc: code whose
+ * device memory belongs to another allocator (a framework's caching pool that has reserved the
+ * GPU) and latency-critical loops in which an allocation or free would synchronize the device.
+ * No counterpart in the reference (its operators allocate every output with torch::zeros).
+ * Same result as svs_tvl1_solve_batch with the plain-load iterate kernel (tile id 6) for the
+ * same parameters; the caller passes device frames I0, I1 [nz,ny,nx] and the flow u_out
+ * [nz,ny,nx,3]. All other device memory the solve needs (pyramid, linearisation, dual state,
+ * descriptors, tile lists) is taken from one static 32 MiB device array that every GPU loading
+ * the library holds until exit; a volume whose state does not fit is rejected with
+ * SVS_ERR_INVALID_ARG (about 56^3 fits with FP32 storage, larger with 16-bit storage). Calls no
+ * cudaMalloc or cudaFree. The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress): make it before any stream capture. Every call reuses the same array
+ * and clears the state it uses, so calls that overlap on the GPU (different streams or devices
+ * sharing nothing else) race and must be serialized by the caller; the p output and the
+ * num_scales == 1 warm start of svs_pair_desc are not offered here. */
+svs_status svs_tvl1_solve_noalloc(const svs_tvl1_params* params, const float* I0, const float* I1,
+                                  int nz, int ny, int nx, float* u_out, svs_stream_t stream);
+
 /* Kernel-launch counter (all kernels this library launched in this process), for benchmarks. */
 uint64_t svs_launch_count(void);
 

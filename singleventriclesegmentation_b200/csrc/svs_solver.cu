@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -937,3 +938,193 @@ svs_status svs_tvl1_plan_check(svs_plan* P) {
 }
 
 }  // extern "C"
+
+// =============================================================================================
+// Allocation-free single-pair solve.
+//
+// For callers that cannot call cudaMalloc: code whose device memory is owned by another
+// allocator (a framework's caching pool that has reserved the GPU), and latency-critical loops
+// in which an allocation or free would synchronize the device. Everything the solve needs
+// beyond the caller's inputs and outputs (pyramid, linearisation, dual state, descriptors and
+// tile lists) is carved out of one file-scope device array of kNoAllocScratchBytes.
+// =============================================================================================
+namespace svs {
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = (size_t)32 << 20;  // 32 MiB, held by every GPU that loads the library
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device: set up once per device (with that
+// device current) through cudaGetSymbolAddress; in host code the array's name is only a host-side
+// stand-in and must never be handed to a kernel.
+svs_status noalloc_scratch(unsigned char** out) {
+  int dev = 0;
+  svs_status st = check_cuda(cudaGetDevice(&dev), "svs_tvl1_solve_noalloc: cudaGetDevice");
+  if (st) return st;
+  if (dev < 0 || dev >= kMaxDevices) return fail(SVS_ERR_UNSUPPORTED, "svs_tvl1_solve_noalloc: device index out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    st = check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "svs_tvl1_solve_noalloc: cudaGetSymbolAddress");
+    if (st) return st;
+    g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return SVS_OK;
+}
+
+}  // namespace
+}  // namespace svs
+
+extern "C" svs_status svs_tvl1_solve_noalloc(const svs_tvl1_params* prm, const float* I0, const float* I1,
+                                             int nz, int ny, int nx, float* u_out, svs_stream_t stream) {
+  using namespace svs;
+  SVS_REQUIRE(prm && I0 && I1 && u_out, "svs_tvl1_solve_noalloc: null pointer");
+  SVS_REQUIRE(prm->num_scales >= 1 && prm->num_scales <= 8, "svs_tvl1_solve_noalloc: num_scales out of range");
+  SVS_REQUIRE(prm->max_warps >= 0 && prm->max_outer_iterations >= 0, "svs_tvl1_solve_noalloc: negative iteration count");
+  SVS_REQUIRE(prm->primaldual_algorithm_type == 1 || prm->primaldual_algorithm_type == 2,
+              "svs_tvl1_solve_noalloc: primaldual_algorithm_type must be 1 or 2");
+  SVS_REQUIRE(prm->boundary >= 0 && prm->boundary <= 2, "svs_tvl1_solve_noalloc: bad boundary type");
+  SVS_REQUIRE(prm->interpolation >= 0 && prm->interpolation <= 2, "svs_tvl1_solve_noalloc: bad interpolation type");
+  SVS_REQUIRE(prm->storage >= 0 && prm->storage <= 4, "svs_tvl1_solve_noalloc: bad storage type");
+  SVS_REQUIRE(prm->weight_tv >= 0.f, "svs_tvl1_solve_noalloc: weight_tv must be >= 0");
+  SVS_REQUIRE(prm->median_kernel == 0 || prm->median_kernel == 1 || prm->median_kernel == 3 ||
+                  prm->median_kernel == 5 || prm->median_kernel == 7,
+              "svs_tvl1_solve_noalloc: median kernel must be 0, 1, 3, 5 or 7");
+  SVS_REQUIRE(nz < 65535 && ny < 65535 && nx < 65535, "svs_tvl1_solve_noalloc: volume dimension too large");
+
+  // A host-only plan: the same launch sequence as svs_tvl1_solve_batch, with every device
+  // pointer carved from the scratch array and the plain-load iterate kernel at every level.
+  svs_plan P;
+  P.prm = *prm;
+  P.num_pairs = 1;
+  P.levels = prm->num_scales;
+  P.dims = {nz, ny, nx};
+  P.h_descs.resize(P.levels);
+  const size_t ub = flow_bytes(prm->storage), sb = field_bytes(prm->storage);
+  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+  size_t bytes = al(P.levels * sizeof(Desc)) + al(7 * sizeof(float*));
+  {
+    int z = nz, y = ny, x = nx;
+    for (int l = 0; l < P.levels; ++l) {
+      if (l > 0) { z = (z + 1) / 2; y = (y + 1) / 2; x = (x + 1) / 2; }
+      SVS_REQUIRE(z >= 3 && y >= 3 && x >= 3,
+                  "svs_tvl1_solve_noalloc: every pyramid level needs at least 3 nodes per axis");
+      Desc& d = P.h_descs[l];
+      std::memset(&d, 0, sizeof(d));
+      d.nz = z; d.ny = y; d.nx = x;
+      d.pitch = (x + 7) / 8 * 8;
+      d.n = (long long)z * y * x;
+      d.cs = (long long)d.pitch * y * z;
+      if (prm->length_type == 0) { d.lz = (float)(z - 1); d.ly = (float)(y - 1); d.lx = (float)(x - 1); }
+      else { d.lz = prm->length_z; d.ly = prm->length_y; d.lx = prm->length_x; }
+      d.hz = d.lz / (float)(z - 1); d.hy = d.ly / (float)(y - 1); d.hx = d.lx / (float)(x - 1);
+      const size_t n = (size_t)d.n, cs = (size_t)d.cs;
+      bytes += 2 * al(n * 4) + al(3 * n * 4) + al(6 * cs * sb) + al(cs * sb) + al(3 * cs * sb) +
+               2 * al(3 * cs * ub) + 2 * al(9 * cs * sb);
+      if (l == 0 && prm->median_kernel > 1) bytes += al(3 * n * 4);
+    }
+  }
+  P.level_tile.assign(P.levels, 6);  // plain-load 32x8
+  P.h_tiles.assign(P.levels, {});
+  for (int l = 0; l < P.levels; ++l) {
+    build_tiles(P, l, 6);
+    bytes += al(P.h_tiles[l].size() * sizeof(Tile));
+  }
+  if (bytes > kNoAllocScratchBytes)
+    return fail(SVS_ERR_INVALID_ARG, "svs_tvl1_solve_noalloc: a " + std::to_string(nz) + "x" + std::to_string(ny) + "x" +
+                                         std::to_string(nx) + " solve needs " + std::to_string(bytes) +
+                                         " bytes of scratch; the allocation-free entry point has " +
+                                         std::to_string(kNoAllocScratchBytes) + " (use svs_tvl1_solve_batch)");
+  unsigned char* base = nullptr;
+  svs_status st = noalloc_scratch(&base);
+  if (st) return st;
+  char* cur = reinterpret_cast<char*>(base);
+  P.d_descs = carve<Desc>(cur, P.levels);
+  float** ptrs = carve<float*>(cur, 7);  // raw I0, raw I1, u_out, p_out, median temp, u_init, p_init
+  P.d_raw = ptrs;
+  P.d_uout = ptrs + 2;
+  P.d_pout = ptrs + 3;
+  P.d_umed = ptrs + 4;
+  P.d_uinit = const_cast<const float**>(ptrs + 5);
+  P.d_pinit = const_cast<const float**>(ptrs + 6);
+  P.d_tiles.assign(P.levels, nullptr);
+  for (int l = 0; l < P.levels; ++l) P.d_tiles[l] = carve<Tile>(cur, P.h_tiles[l].size());
+  char* state_begin = cur;
+  for (int l = 0; l < P.levels; ++l) {
+    Desc& d = P.h_descs[l];
+    const size_t n = (size_t)d.n, cs = (size_t)d.cs;
+    d.I0 = carve<float>(cur, n);
+    d.I1 = carve<float>(cur, n);
+    d.g1 = carve<float>(cur, 3 * n);
+    d.D = carve<char>(cur, 6 * cs * sb);
+    d.rc = carve<char>(cur, cs * sb);
+    d.gw = carve<char>(cur, 3 * cs * sb);
+    d.u[0] = carve<char>(cur, 3 * cs * ub);
+    d.u[1] = carve<char>(cur, 3 * cs * ub);
+    d.p[0] = carve<char>(cur, 9 * cs * sb);
+    d.p[1] = carve<char>(cur, 9 * cs * sb);
+  }
+  float* umed = prm->median_kernel > 1 ? carve<float>(cur, 3 * (size_t)nz * ny * nx) : nullptr;
+  // The blur reads the caller's frames and finalize writes the caller's flow directly.
+  P.raw = {const_cast<float*>(I0), const_cast<float*>(I1)};
+  P.uout = {u_out};
+  P.umed = {umed};
+  P.pout = {nullptr};
+  std::vector<float*> hp = {P.raw[0], P.raw[1], u_out, nullptr, umed, nullptr, nullptr};
+  // step-size schedule and blur weights exactly as svs_tvl1_plan_create builds them
+  {
+    double sg = prm->sigma, ta = prm->tau;
+    for (int it = 0; it < prm->max_outer_iterations; ++it) {
+      P.sig_sched.push_back((float)sg);
+      P.tau_sched.push_back((float)ta);
+      if (prm->primaldual_algorithm_type == 2) {
+        const double th = 1.0 / std::sqrt(1.0 + 2.0 * prm->gamma * ta);
+        ta *= th;
+        sg /= th;
+      }
+    }
+  }
+  if (prm->use_gaussian_blur) {
+    const double sgm = prm->gaussian_blur_sigma;
+    int ks = (int)(sgm * 5);
+    if (ks % 2 == 0) ks += 1;
+    SVS_REQUIRE(ks <= 9 && ks >= 1, "svs_tvl1_solve_noalloc: gaussian_blur_sigma out of range (kernel size <= 9)");
+    const int lo = -((ks + 1) / 2), hi = ks / 2 + 1;
+    std::vector<float> t(ks), g(ks), k1(ks);
+    for (int i = 0; i < ks; ++i) t[i] = (ks == 1) ? (float)lo : (float)(lo + (double)(hi - lo) * i / (ks - 1));
+    float gs = 0.f;
+    for (int i = 0; i < ks; ++i) {
+      const float a = t[i] / (float)sgm;
+      g[i] = std::exp(-(a * a) / 2.0f);
+      gs += g[i];
+    }
+    for (int i = 0; i < ks; ++i) k1[i] = g[i] / gs;
+    float tot = 0.f;
+    std::vector<float> k3((size_t)ks * ks * ks);
+    for (int a = 0; a < ks; ++a)
+      for (int b = 0; b < ks; ++b)
+        for (int c = 0; c < ks; ++c) { k3[(a * ks + b) * ks + c] = k1[a] * k1[b] * k1[c]; tot += k3[(a * ks + b) * ks + c]; }
+    for (size_t i = 0; i < k3.size(); ++i) P.blur.w[i] = k3[i] / tot;
+    P.blur_r = ks / 2;
+  }
+  // Metadata into the scratch (pageable sources: each copy returns once the data is staged),
+  // then clear the state region so no value from an earlier call is ever read.
+  cudaStream_t s = stream;
+  st = check_cuda(cudaMemcpyAsync(P.d_descs, P.h_descs.data(), P.levels * sizeof(Desc), cudaMemcpyHostToDevice, s), "svs_tvl1_solve_noalloc");
+  if (!st) st = check_cuda(cudaMemcpyAsync(ptrs, hp.data(), hp.size() * sizeof(float*), cudaMemcpyHostToDevice, s), "svs_tvl1_solve_noalloc");
+  for (int l = 0; l < P.levels && !st; ++l)
+    st = check_cuda(cudaMemcpyAsync(P.d_tiles[l], P.h_tiles[l].data(), P.h_tiles[l].size() * sizeof(Tile),
+                                    cudaMemcpyHostToDevice, s), "svs_tvl1_solve_noalloc");
+  if (!st) st = check_cuda(cudaMemsetAsync(state_begin, 0, (size_t)(cur - state_begin), s), "svs_tvl1_solve_noalloc");
+  if (st) return st;
+  P.warm = false;
+  const long long nl = enqueue(P, s);
+  if (nl < 0) return fail(SVS_ERR_LAUNCH, std::string("svs_tvl1_solve_noalloc: launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+  count_launches((uint64_t)nl);
+  return SVS_OK;
+}
