@@ -9,6 +9,8 @@ from __future__ import annotations
 
 import json
 import os
+
+import numpy as np
 from typing import Dict, List, Optional, Sequence, Tuple
 
 import torch
@@ -91,3 +93,54 @@ def tune(plan: SolverPlan, storage: str, levels: int, candidates: Optional[Seque
     if use_cache:
         _store(db)
     return chosen
+
+
+def _main(argv=None) -> None:
+    """Time the iterate-kernel variants on a batch of identical synthetic pairs:
+
+        python -m singleventriclesegmentation_b200.autotune --pairs 16 --size 80 --storage f32 --tiles 1,2
+
+    Each variant: one short solve (1 warp x 10 iterations per level) to fill the state, then the
+    mean time of level-0 iterate launches; prints one JSON line per variant."""
+    import argparse
+    import json as _json
+
+    from . import synthetic
+    from .tvl13d import TVL13DOpticalFlow
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--pairs", type=int, default=16)
+    ap.add_argument("--size", type=int, default=80)
+    ap.add_argument("--storage", default="f32")
+    ap.add_argument("--tiles", default="")
+    ap.add_argument("--iters", type=int, default=20)
+    ap.add_argument("--level", type=int, default=0)
+    args = ap.parse_args(argv)
+    dev = torch.device("cuda", 0)
+    shape = (args.size,) * 3
+    I0, I1, _ = synthetic.frame_pair(shape, seed=0, device="cuda")
+    I0, I1 = torch.from_numpy(I0).to(dev), torch.from_numpy(I1).to(dev)
+    tiles = [int(t) for t in args.tiles.split(",") if t] or list(range(1, int(_lib.lib().svs_tvl1_num_tiles()) + 1))
+    bpv = {"f32": 136, "bf16": 68, "f16": 68, "bf16-flow32": 80, "f16-flow32": 80}[args.storage]
+    for tid in tiles:
+        s = TVL13DOpticalFlow(3, 1, 10, 1.0, 0.025, 2, (0.5, 0.5, 0.25, 1.0), True, (5.0, 0.5), True, 1.0,
+                              "CUBIC_HERMITESPLINE", "MIRROR", "numDofs", (1, 1, 1), dev, storage=args.storage)
+        s.tile_id = tid
+        try:
+            plan = s.plan_for([shape] * args.pairs)
+            outs = [torch.empty(shape + (3,), device=dev) for _ in range(args.pairs)]
+            plan.solve([I0] * args.pairs, [I1] * args.pairs, outs)
+            torch.cuda.synchronize()
+            plan.check()
+            ms = time_variant(plan, args.level, tid, args.iters)
+            plan.check()
+            vox = args.pairs * int(np.prod([(n + (1 << args.level) - 1) >> args.level for n in shape]))
+            print(_json.dumps({"storage": args.storage, "tile": tid, "level": args.level, "ms": round(ms, 4),
+                               "GBs": round(vox * bpv / (ms / 1e3) / 1e9, 1)}), flush=True)
+            plan.close()
+        except _lib.SVSError as e:
+            print(_json.dumps({"storage": args.storage, "tile": tid, "error": str(e)[:160]}), flush=True)
+
+
+if __name__ == "__main__":
+    _main()

@@ -49,13 +49,17 @@ __device__ __forceinline__ Stencil3 adj_coef(int i, int n, int bdry, float ih) {
   return {0.f, -a, -a};
 }
 
+// GEN = false: MIRROR boundary, where every stencil has a zero centre coefficient (the centre
+// term is dropped; for h = 1 the result is bitwise that of the three-term form).
+template <bool GEN>
 __device__ __forceinline__ float apply3(const Stencil3& s, float prev, float cur, float next) {
-  return fmaf(s.p, next, fmaf(s.c, cur, s.m * prev));
+  if (GEN) return fmaf(s.p, next, fmaf(s.c, cur, s.m * prev));
+  return fmaf(s.p, next, s.m * prev);
 }
 
 // Dual update of one flow component at one voxel, tvl13d.py:215-222 with
 // opticalFlowOps.cu:179-208: v = p + sigma D g; p_new = v / max(1, |v| / weight_tv), written as
-// v * min(1, weight_tv * rsqrt(|v|^2)). weight_tv == 0 zeroes p (tvl13d.py:223-224).
+// v * min(1, weight_tv * rsqrt(|v|^2)).
 __device__ __forceinline__ void dual_row(const float D[6], float ex, float ey, float ez, float& p0,
                                          float& p1, float& p2, float sigma, float wtv, float wtv2) {
   const float d0 = D[0] * ex + D[1] * ey + D[2] * ez;
@@ -63,14 +67,11 @@ __device__ __forceinline__ void dual_row(const float D[6], float ex, float ey, f
   const float d2 = D[2] * ex + D[4] * ey + D[5] * ez;
   const float v0 = p0 + sigma * d0, v1 = p1 + sigma * d1, v2 = p2 + sigma * d2;
   const float nsq = v0 * v0 + v1 * v1 + v2 * v2;
+  // weight_tv == 0 gives sc = 0 (or v = 0), i.e. p = 0 as tvl13d.py:223-224 requires
   const float sc = (nsq > wtv2) ? wtv * rsqrtf(nsq) : 1.0f;
-  if (wtv > 0.f) {
-    p0 = v0 * sc;
-    p1 = v1 * sc;
-    p2 = v2 * sc;
-  } else {
-    p0 = p1 = p2 = 0.f;
-  }
+  p0 = v0 * sc;
+  p1 = v1 * sc;
+  p2 = v2 * sc;
 }
 
 // Primal update at one voxel, tvl13d.py:229-235 with opticalFlowOps.cu:123-175:
@@ -81,22 +82,17 @@ __device__ __forceinline__ void primal_voxel(const float u[3], const float div[3
   const float g2s = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
 #pragma unroll
   for (int c = 0; c < 3; ++c) un[c] = u[c] - tau * div[c];
+  // the three cases of opticalFlowOps.cu:140-171 as one step length along g (no divergence):
+  // rho < -th: +factor; rho > th: -factor; |rho| <= th: -rho/|g|^2 (0 where |g|^2 <= 1e-10,
+  // the reference's (double)g2 > 1e-10 for a float g2)
   const float th = factor * g2s;
-  if (rho < -th) {
+  const float t = (rho < -th) ? factor : (rho > th) ? -factor : (g2s >= 1e-10f ? __fdividef(-rho, g2s) : 0.f);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) un[c] += factor * g[c];
-  } else if (rho > th) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) un[c] -= factor * g[c];
-  } else if (g2s >= 1e-10f) {  // the reference's (double)g2 > 1e-10 for a float g2
-    const float t = __fdividef(-rho, g2s);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) un[c] += t * g[c];
-  }
+  for (int c = 0; c < 3; ++c) un[c] = fmaf(t, g[c], un[c]);
 }
 
 // ------------------------------------------------------------------------ plain-load form
-template <typename SU, typename SP, int TX, int TY>
+template <typename SU, typename SP, int TX, int TY, bool GEN>
 __global__ void __launch_bounds__((TX + 2) * (TY + 2))
 iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, IterArgs a) {
   constexpr int PX = TX + 2, PY = TY + 2, UX = TX + 4, UY = TY + 4;
@@ -193,9 +189,9 @@ iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, I
       const Stencil3 fz = fwd_coef(k, nz, bdry, Dg.hz);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const float ex = apply3(fx, su[slot][c][ty + 1][tx], uc[c], su[slot][c][ty + 1][tx + 2]);
-        const float ey = apply3(fy, su[slot][c][ty][tx + 1], uc[c], su[slot][c][ty + 2][tx + 1]);
-        const float ez = apply3(fz, um[c], uc[c], up[c]);
+        const float ex = apply3<GEN>(fx, su[slot][c][ty + 1][tx], uc[c], su[slot][c][ty + 1][tx + 2]);
+        const float ey = apply3<GEN>(fy, su[slot][c][ty][tx + 1], uc[c], su[slot][c][ty + 2][tx + 1]);
+        const float ez = apply3<GEN>(fz, um[c], uc[c], up[c]);
         dual_row(Dk, ex, ey, ez, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2], a.sigma, a.wtv, wtv2);
       }
       if (interior && k >= z0 && k < z1) {
@@ -216,9 +212,9 @@ iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, I
       float div[3], un[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const float dx = apply3(ax, sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1]);
-        const float dy = apply3(ay, sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx]);
-        div[c] = (dx + dy) + apply3(az, qzmm[c], qzm[c], qzc[c]);
+        const float dx = apply3<GEN>(ax, sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1]);
+        const float dy = apply3<GEN>(ay, sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx]);
+        div[c] = (dx + dy) + apply3<GEN>(az, qzmm[c], qzm[c], qzc[c]);
       }
       primal_voxel(um, div, a.tau, a.factor, rcj, gj, un);
       const int o = j * plane + col;
@@ -251,9 +247,9 @@ iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, I
       for (int c = 0; c < 3; ++c) gj[c] = Store<SP>::ld(gwm + c * cs + o);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const float dx = apply3(ax, sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1]);
-        const float dy = apply3(ay, sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx]);
-        div[c] = (dx + dy) + apply3(az, qzmm[c], qzm[c], 0.f);
+        const float dx = apply3<GEN>(ax, sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1]);
+        const float dy = apply3<GEN>(ay, sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx]);
+        div[c] = (dx + dy) + apply3<GEN>(az, qzmm[c], qzm[c], 0.f);
       }
       primal_voxel(um, div, a.tau, a.factor, rcj, gj, un);
 #pragma unroll
@@ -313,6 +309,9 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, u
 
 __host__ __device__ constexpr int round_up_c(int v, int m) { return (v + m - 1) / m * m; }
 
+__device__ __forceinline__ int gx_of(const Tile& T, int tid, int px) { return T.x0 - 1 + tid % px; }
+__device__ __forceinline__ int gy_of(const Tile& T, int tid, int px) { return T.y0 - 1 + tid / px; }
+
 // Shared-memory geometry of the TMA form: flow stored as SU, the rest as SP, tile TX x TY,
 // prefetch distance DIST planes.
 //   u ring    DIST+2 slots: planes k-1, k, k+1 are read at step k;
@@ -353,7 +352,7 @@ struct TmaGeom {
   static constexpr int FULL_TX = U_TX + P_TX + D_TX + RC_TX + GW_TX;
 };
 
-template <typename SU, typename SP, int TX, int TY, int DIST>
+template <typename SU, typename SP, int TX, int TY, int DIST, bool GEN>
 __global__ void __launch_bounds__((TX + 2) * (TY + 2))
 iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs,
                    const TMaps* __restrict__ maps, IterArgs a, int* __restrict__ status) {
@@ -372,8 +371,9 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
   const int cs = (int)Dg.cs;
   const int plane = Dg.pitch * ny;
   const int z0 = T.z0z1 & 0xffff, z1 = T.z0z1 >> 16;
-  SU* __restrict__ u_dst = reinterpret_cast<SU*>(Dg.u[a.src ^ 1]);
-  SP* __restrict__ p_dst = reinterpret_cast<SP*>(Dg.p[a.src ^ 1]);
+  const int col0 = gy_of(T, threadIdx.x, G::PX) * Dg.pitch + gx_of(T, threadIdx.x, G::PX);
+  SU* __restrict__ u_dst = reinterpret_cast<SU*>(Dg.u[a.src ^ 1]) + col0;  // this thread's column
+  SP* __restrict__ p_dst = reinterpret_cast<SP*>(Dg.p[a.src ^ 1]) + col0;
   const CUtensorMap* mu = &M->u[a.src];
   const CUtensorMap* mp = &M->p[a.src];
 
@@ -384,7 +384,6 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
   const bool corner = (tx == 0 || tx == PX - 1) && (ty == 0 || ty == PY - 1);
   const bool dual_on = in_dom && !corner;
   const bool interior = in_dom && tx >= 1 && tx <= TX && ty >= 1 && ty <= TY;
-  const int col = gy * Dg.pitch + gx;
   const int uo = (ty + 1) * UXB + (tx + AU - 1);  // own column in a u box component
   const int po = ty * PXB + (tx + AP - 1);        // own column in a p/D box component
   const int ro = (ty - 1) * TX + (tx - 1);        // own column in an rc/gw box (interior)
@@ -435,6 +434,7 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
   bool bad = false;
 
   float qzmm[3] = {0.f, 0.f, 0.f}, qzm[3] = {0.f, 0.f, 0.f}, qzc[3] = {0.f, 0.f, 0.f};
+  float uown_m[3] = {0.f, 0.f, 0.f}, uown_c[3] = {0.f, 0.f, 0.f}, uown_p[3] = {0.f, 0.f, 0.f};
   const float wtv2 = a.wtv * a.wtv;
 
   for (int k = kb; k <= ke; ++k) {
@@ -445,10 +445,18 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
       if (!mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1))) bad = true;
     }
     const int qs = k % 3;
+    // own column of u: planes k-1 and k from the previous step, k+1 read once here
+    if (k == kb) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        uown_m[c] = (k - 1 >= pl) ? Store<SU>::sh(ubox(k - 1) + uo + c * UYB * UXB) : 0.f;
+        uown_c[c] = Store<SU>::sh(ubox(k) + uo + c * UYB * UXB);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) uown_p[c] = (k + 1 <= ph) ? Store<SU>::sh(ubox(k + 1) + uo + c * UYB * UXB) : 0.f;
     if (dual_on && !bad) {
       const SU* Uk = ubox(k) + uo;
-      const SU* Um = (k - 1 >= pl) ? ubox(k - 1) + uo : Uk;  // coefficient 0 where absent
-      const SU* Up = (k + 1 <= ph) ? ubox(k + 1) + uo : Uk;
       const unsigned char* PD = smem + G::PD_OFF + ((k - kb) % G::NPD) * G::PD_SLOT;
       const SP* P = reinterpret_cast<const SP*>(PD) + po;
       const SP* Dm = reinterpret_cast<const SP*>(PD + G::P_SLOT) + po;
@@ -461,14 +469,14 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const SU* u = Uk + c * UYB * UXB;
-        const float uc = Store<SU>::sh(u);
-        const float ex = apply3(fx, Store<SU>::sh(u - 1), uc, Store<SU>::sh(u + 1));
-        const float ey = apply3(fy, Store<SU>::sh(u - UXB), uc, Store<SU>::sh(u + UXB));
-        const float ez = apply3(fz, Store<SU>::sh(Um + c * UYB * UXB), uc, Store<SU>::sh(Up + c * UYB * UXB));
+        const float uc = uown_c[c];
+        const float ex = apply3<GEN>(fx, Store<SU>::sh(u - 1), uc, Store<SU>::sh(u + 1));
+        const float ey = apply3<GEN>(fy, Store<SU>::sh(u - UXB), uc, Store<SU>::sh(u + UXB));
+        const float ez = apply3<GEN>(fz, uown_m[c], uc, uown_p[c]);
         dual_row(Dk, ex, ey, ez, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2], a.sigma, a.wtv, wtv2);
       }
       if (interior && k >= z0 && k < z1) {
-        SP* dst = p_dst + k * plane + col;
+        SP* dst = p_dst + k * plane;
 #pragma unroll
         for (int c = 0; c < 9; ++c) Store<SP>::st(dst + c * cs, pk[c]);
       }
@@ -494,20 +502,18 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
       const unsigned char* R = smem + G::R_OFF + ((j - kb) % G::NR) * G::R_SLOT;
       const SP* RC = reinterpret_cast<const SP*>(R) + ro;
       const SP* GW = reinterpret_cast<const SP*>(R + G::RC_SLOT) + ro;
-      const SU* Uj = ubox(j) + uo;
       const Stencil3 az = adj_coef(j, nz, bdry, ihz);
       const float rcj = Store<SP>::sh(RC);
-      float gj[3], uj[3], div[3], un[3];
+      float gj[3], div[3], un[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         gj[c] = Store<SP>::sh(GW + c * TY * TX);
-        uj[c] = Store<SU>::sh(Uj + c * UYB * UXB);
-        const float dx = apply3(ax, sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1]);
-        const float dy = apply3(ay, sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx]);
-        div[c] = (dx + dy) + apply3(az, qzmm[c], qzm[c], qzc[c]);
+        const float dx = apply3<GEN>(ax, sq[ps][c][ty][tx - 1], GEN ? sq[ps][c][ty][tx] : 0.f, sq[ps][c][ty][tx + 1]);
+        const float dy = apply3<GEN>(ay, sq[ps][3 + c][ty - 1][tx], GEN ? sq[ps][3 + c][ty][tx] : 0.f, sq[ps][3 + c][ty + 1][tx]);
+        div[c] = (dx + dy) + apply3<GEN>(az, qzmm[c], qzm[c], qzc[c]);
       }
-      primal_voxel(uj, div, a.tau, a.factor, rcj, gj, un);
-      SU* dst = u_dst + j * plane + col;
+      primal_voxel(uown_m, div, a.tau, a.factor, rcj, gj, un);
+      SU* dst = u_dst + j * plane;
 #pragma unroll
       for (int c = 0; c < 3; ++c) Store<SU>::st(dst + c * cs, un[c]);
     }
@@ -515,6 +521,8 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
     for (int c = 0; c < 3; ++c) {
       qzmm[c] = qzm[c];
       qzm[c] = qzc[c];
+      uown_m[c] = uown_c[c];
+      uown_c[c] = uown_p[c];
     }
   }
   if (bad) {
@@ -535,20 +543,18 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
       const unsigned char* R = smem + G::R_OFF + ((j - kb) % G::NR) * G::R_SLOT;
       const SP* RC = reinterpret_cast<const SP*>(R) + ro;
       const SP* GW = reinterpret_cast<const SP*>(R + G::RC_SLOT) + ro;
-      const SU* Uj = ubox(j) + uo;
       const Stencil3 az = adj_coef(j, nz, bdry, ihz);
       const float rcj = Store<SP>::sh(RC);
-      float gj[3], uj[3], div[3], un[3];
+      float gj[3], div[3], un[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         gj[c] = Store<SP>::sh(GW + c * TY * TX);
-        uj[c] = Store<SU>::sh(Uj + c * UYB * UXB);
-        const float dx = apply3(ax, sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1]);
-        const float dy = apply3(ay, sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx]);
-        div[c] = (dx + dy) + apply3(az, qzmm[c], qzm[c], 0.f);
+        const float dx = apply3<GEN>(ax, sq[ps][c][ty][tx - 1], GEN ? sq[ps][c][ty][tx] : 0.f, sq[ps][c][ty][tx + 1]);
+        const float dy = apply3<GEN>(ay, sq[ps][3 + c][ty - 1][tx], GEN ? sq[ps][3 + c][ty][tx] : 0.f, sq[ps][3 + c][ty + 1][tx]);
+        div[c] = (dx + dy) + apply3<GEN>(az, qzmm[c], qzm[c], 0.f);
       }
-      primal_voxel(uj, div, a.tau, a.factor, rcj, gj, un);
-      SU* dst = u_dst + j * plane + col;
+      primal_voxel(uown_m, div, a.tau, a.factor, rcj, gj, un);
+      SU* dst = u_dst + j * plane;
 #pragma unroll
       for (int c = 0; c < 3; ++c) Store<SU>::st(dst + c * cs, un[c]);
     }

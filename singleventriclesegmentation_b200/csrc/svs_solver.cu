@@ -446,8 +446,10 @@ template <typename SU, typename SP, int TX, int TY, int DIST>
 bool tma_prepare(svs_plan& P, std::vector<TMaps>& maps, int level) {
   using G = TmaGeom<SU, SP, TX, TY, DIST>;
   if (G::SMEM > 227 * 1024) return false;
-  if (cudaFuncSetAttribute(iterate_tma_kernel<SU, SP, TX, TY, DIST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           G::SMEM) != cudaSuccess) {
+  if (cudaFuncSetAttribute(iterate_tma_kernel<SU, SP, TX, TY, DIST, false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM) != cudaSuccess ||
+      cudaFuncSetAttribute(iterate_tma_kernel<SU, SP, TX, TY, DIST, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
@@ -460,16 +462,24 @@ bool iter_variant(svs_plan& P, std::vector<TMaps>* maps, int level, int tid, int
                   cudaStream_t s) {
   const unsigned nt = (unsigned)P.h_tiles[level].size();
   const Tile* tl = P.d_tiles.empty() ? nullptr : P.d_tiles[level];
+  // the MIRROR boundary (the solver's default) gets two-term stencils; other boundaries the
+  // general three-term form
+  const bool gen = P.prm.boundary != SVS_BOUNDARY_MIRROR;
 #define SVS_TMA_CASE(ID, TX, TY, DS)                                                                      \
   case ID:                                                                                                \
     if (op == 0) return tma_prepare<SU, SP, TX, TY, DS>(P, *maps, level);                                \
-    iterate_tma_kernel<SU, SP, TX, TY, DS><<<nt, (TX + 2) * (TY + 2), TmaGeom<SU, SP, TX, TY, DS>::SMEM, s>>>( \
-        tl, P.d_descs, P.d_maps, *a, P.d_status);                                                         \
+    if (gen)                                                                                              \
+      iterate_tma_kernel<SU, SP, TX, TY, DS, true><<<nt, (TX + 2) * (TY + 2), TmaGeom<SU, SP, TX, TY, DS>::SMEM, s>>>( \
+          tl, P.d_descs, P.d_maps, *a, P.d_status);                                                       \
+    else                                                                                                  \
+      iterate_tma_kernel<SU, SP, TX, TY, DS, false><<<nt, (TX + 2) * (TY + 2), TmaGeom<SU, SP, TX, TY, DS>::SMEM, s>>>( \
+          tl, P.d_descs, P.d_maps, *a, P.d_status);                                                       \
     return true;
 #define SVS_PLAIN_CASE(ID, TX, TY)                                                                   \
   case ID:                                                                                           \
     if (op == 0) return true;                                                                        \
-    iterate_kernel<SU, SP, TX, TY><<<nt, (TX + 2) * (TY + 2), 0, s>>>(tl, P.d_descs, *a);            \
+    if (gen) iterate_kernel<SU, SP, TX, TY, true><<<nt, (TX + 2) * (TY + 2), 0, s>>>(tl, P.d_descs, *a); \
+    else iterate_kernel<SU, SP, TX, TY, false><<<nt, (TX + 2) * (TY + 2), 0, s>>>(tl, P.d_descs, *a); \
     return true;
   switch (tid) {
     SVS_TMA_CASE(1, 32, 8, 2)
