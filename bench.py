@@ -137,12 +137,15 @@ def oracle_sample(threads: int):
     o.build()
     o.set_threads(threads)
     I0, I1, _ = synthetic.frame_pair(SHAPE, seed=0)
-    # calibrate the iteration count so that the sample is about 10 s of host work
-    probe = 8
-    t0 = time.perf_counter()
-    o.tvl1_compute(I0, I1, o.SolverParams(max_warps=1, max_outer_iterations=probe), dtype=np.float32)
-    per_it = (time.perf_counter() - t0) / probe
-    k = int(min(4500, max(probe, 10.0 / max(per_it, 1e-6))))
+    # calibrate the iteration count so that the sample is about 15 s of host work: two probes
+    # separate the fixed cost (blur, pyramid, linearisation) from the per-iteration cost
+    times = []
+    for probe in (4, 36):
+        t0 = time.perf_counter()
+        o.tvl1_compute(I0, I1, o.SolverParams(max_warps=1, max_outer_iterations=probe), dtype=np.float32)
+        times.append(time.perf_counter() - t0)
+    per_it = max((times[1] - times[0]) / 32, 1e-6)
+    k = int(min(4500, max(36, 15.0 / per_it)))
     P = o.SolverParams(max_warps=1, max_outer_iterations=k)
     t0 = time.perf_counter()
     o.tvl1_compute(I0, I1, P, dtype=np.float32)
