@@ -185,12 +185,19 @@ svs_status svs_tvl1_plan_destroy(svs_plan* plan);
 /* Bytes of device memory the plan holds. */
 size_t svs_tvl1_plan_device_bytes(const svs_plan* plan);
 /* Select the iterate-kernel variant (0 = automatic) for later solves; SVS_ERR_INVALID_ARG for an
- * unknown id. Variants 1-5 are TMA pipelines (tile x prefetch distance: 32x8/2, 32x8/3, 64x4/2, 16x16/2, 32x16/2),
- * 6-8 plain-load forms (32x8, 32x4, 16x16). Used by the autotuner. */
+ * unknown id. Variants 1-5 are TMA pipelines (tile x prefetch distance: 32x8/2, 32x8/3, 64x4/2,
+ * 16x16/2, 32x16/2), 6-8 plain-load forms (32x8, 32x4, 16x16), 9-20 split-role TMA pipelines
+ * (interior, halo-row and halo-column lanes in separate warps; svs_tvl1_tile_info gives each
+ * shape). Used by the autotuner. */
 svs_status svs_tvl1_plan_set_tile(svs_plan* plan, int tile_id);
 /* Same for one pyramid level only (0 = fall back to the plan-wide choice). */
 svs_status svs_tvl1_plan_set_level_tile(svs_plan* plan, int level, int tile_id);
 int svs_tvl1_num_tiles(void);
+/* Shape of variant tile_id: tile width and height, prefetch distance, form (0 plain-load, 1 TMA
+ * pipeline, 2 split-role TMA pipeline) and voxels per lane (1 or 2); any output may be NULL;
+ * SVS_ERR_INVALID_ARG for an unknown id. No counterpart in the reference (a query for the
+ * autotuner and tests). */
+svs_status svs_tvl1_tile_info(int tile_id, int* tx, int* ty, int* dist, int* form, int* lane_voxels);
 
 /* Solve every pair of the plan (pairs[i] must match dims[i] of the plan). */
 svs_status svs_tvl1_solve_batch(svs_plan* plan, const svs_pair_desc* pairs_host, int num_pairs,

@@ -71,6 +71,8 @@ _SIGS = {
     "svs_tvl1_plan_set_tile": (c_int, [c_void_p, c_int]),
     "svs_tvl1_plan_set_level_tile": (c_int, [c_void_p, c_int, c_int]),
     "svs_tvl1_num_tiles": (c_int, []),
+    "svs_tvl1_tile_info": (c_int, [c_int, ctypes.POINTER(c_int), ctypes.POINTER(c_int), ctypes.POINTER(c_int),
+                                   ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
     "svs_tvl1_solve_batch": (c_int, [c_void_p, ctypes.POINTER(PairDesc), c_int, c_void_p]),
     "svs_tvl1_bench_iterations": (c_int, [c_void_p, c_int, c_int, c_void_p]),
     "svs_tvl1_plan_graph_kernels": (ctypes.c_uint64, [c_void_p]),
@@ -129,3 +131,12 @@ def ptr(t: torch.Tensor) -> int:
 
 def launch_count() -> int:
     return int(lib().svs_launch_count())
+
+
+def tile_info(tile_id: int) -> dict:
+    """Shape of an iterate-kernel variant: {"tx", "ty", "dist", "form", "lane_voxels"} with form
+    "plain", "tma" or "split"."""
+    v = [ctypes.c_int() for _ in range(5)]
+    check(lib().svs_tvl1_tile_info(int(tile_id), *[ctypes.byref(x) for x in v]))
+    return {"tx": v[0].value, "ty": v[1].value, "dist": v[2].value,
+            "form": ("plain", "tma", "split")[v[3].value], "lane_voxels": v[4].value}

@@ -30,10 +30,17 @@ def _level_dims(dims: Sequence[Tuple[int, int, int]], levels: int) -> List[List[
     return out
 
 
+def _variants_signature() -> str:
+    """The compiled variant table, so that a cache written by another build is not reused."""
+    n = int(_lib.lib().svs_tvl1_num_tiles())
+    return ",".join("{tx}x{ty}/{dist}{f}{lane_voxels}".format(f=i["form"][0], **i)
+                    for i in map(_lib.tile_info, range(1, n + 1)))
+
+
 def _key(device, storage: str, level_dims) -> str:
     name = torch.cuda.get_device_name(device).replace(" ", "_")
     sig = ";".join("x".join(map(str, d)) for d in level_dims)
-    return f"{name}|{storage}|{sig}"
+    return f"{name}|{_variants_signature()}|{storage}|{sig}"
 
 
 def _load() -> Dict[str, int]:

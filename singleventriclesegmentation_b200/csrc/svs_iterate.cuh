@@ -23,6 +23,8 @@
 //                                              differentialOps.cu:658-1039 (then /h)
 #pragma once
 
+#include <type_traits>
+
 #include "svs_state.cuh"
 
 namespace svs {
@@ -560,5 +562,439 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
     }
   }
 }
+
+// ------------------------------------------------------------------- split-role TMA form
+// The TMA pipeline and tensor maps of iterate_tma_kernel (same boxes), with a different division
+// of work: a lane owns V (1 or 2) x-adjacent voxels (for V = 2 read and written as one 8-byte
+// f32 or 4-byte 16-bit access), and the lanes are split by role:
+//   role 0  interior         TY rows x TX/V lanes (whole warps): dual, p store, q rows, primal,
+//                            u store;
+//   role 1  halo rows        rows y0-1 and y0+TY, TX/V lanes each: dual and the y-row of q;
+//   role 2  halo columns     x0-1 and x0+TX, TY voxels each, one per lane: dual and the x-row
+//                            of q.
+// One __syncthreads per plane, at the END of step k: step k computes the dual of plane k and the
+// primal of plane k-1 (whose x/y rows of q were published before the barrier of step k-1 and
+// whose z-neighbour q(k) is in the lane's registers), so the two are independent within the
+// step; u of planes k-1, k, k+1 is read from the ring. After the barrier, plane k+DIST is issued
+// into the slots of planes k-1 (u, rc/gw) and k (p/D), which nobody reads any more; q rows need
+// two slots (plane k written, plane k-1 read).
+// The arithmetic of every voxel is the expression sequence of iterate_tma_kernel, so the two
+// kernels give bitwise the same result. q rows live in qx [TY][TX+4] (x from x0-2, so V-voxel
+// groups start on even indices) and qy [TY+2][TX] (rows from y0-1).
+template <int V, typename S> struct Lane;
+template <typename S> struct Lane<1, S> {
+  static __device__ __forceinline__ void sh(const S* p, float (&o)[1]) { o[0] = Store<S>::sh(p); }
+  static __device__ __forceinline__ void st(S* p, const float (&v)[1]) { Store<S>::st(p, v[0]); }
+};
+template <typename S> struct Lane<2, S> {
+  static __device__ __forceinline__ void sh(const S* p, float (&o)[2]) {
+    const float2 t = Pair<S>::sh(p);
+    o[0] = t.x;
+    o[1] = t.y;
+  }
+  static __device__ __forceinline__ void st(S* p, const float (&v)[2]) { Pair<S>::st(p, v[0], v[1]); }
+};
+template <> struct Lane<1, float> {
+  static __device__ __forceinline__ void sh(const float* p, float (&o)[1]) { o[0] = *p; }
+  static __device__ __forceinline__ void st(float* p, const float (&v)[1]) { *p = v[0]; }
+};
+template <> struct Lane<2, float> {
+  static __device__ __forceinline__ void sh(const float* p, float (&o)[2]) {
+    const float2 t = *reinterpret_cast<const float2*>(p);
+    o[0] = t.x;
+    o[1] = t.y;
+  }
+  static __device__ __forceinline__ void st(float* p, const float (&v)[2]) {
+    *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+  }
+};
+
+template <typename SU, typename SP, int TX, int TY, int DIST, int V>
+struct SplitGeom {
+  using B = TmaGeom<SU, SP, TX, TY, DIST>;  // box shapes (shared with the tensor maps)
+  static_assert(V == 1 || V == 2, "one or two voxels per lane");
+  static_assert(TX % V == 0, "whole lanes per row");
+  static constexpr int PW = TX / V;          // lanes per row
+  static constexpr int NI = PW * TY;         // role 0 lanes
+  static constexpr int NH = 2 * PW;          // role 1 lanes
+  static constexpr int NC = 2 * TY;          // role 2 lanes
+  static constexpr int NT = NI + NH + NC;
+  static_assert(NI % 32 == 0, "role 0 fills whole warps");
+  static constexpr int NU = DIST + 1, NPD = DIST, NR = DIST + 1, NB = DIST + 1;
+  static constexpr int U_OFF = 0;
+  static constexpr int PD_OFF = U_OFF + NU * B::U_SLOT;
+  static constexpr int R_OFF = PD_OFF + NPD * B::PD_SLOT;
+  static constexpr int SXW = TX + 4;
+  static constexpr int SQX_OFF = R_OFF + NR * B::R_SLOT;
+  static constexpr int SQX_BYTES = 2 * 3 * TY * SXW * 4;
+  static constexpr int SQY_OFF = SQX_OFF + SQX_BYTES;
+  static constexpr int SQY_BYTES = 2 * 3 * (TY + 2) * TX * 4;
+  static constexpr int BAR_OFF = round_up_c(SQY_OFF + SQY_BYTES, 8);
+  static constexpr int SMEM = BAR_OFF + NB * 8;
+};
+
+template <typename SU, typename SP, int TX, int TY, int DIST, int V, int MINB, bool GEN>
+__global__ void __launch_bounds__(SplitGeom<SU, SP, TX, TY, DIST, V>::NT, MINB)
+iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs,
+                     const TMaps* __restrict__ maps, IterArgs a, int* __restrict__ status) {
+  using G = SplitGeom<SU, SP, TX, TY, DIST, V>;
+  using B = typename G::B;
+  constexpr int AU = B::AU, AP = B::AP, UXB = B::UXB, PXB = B::PXB;
+  constexpr int UC = B::UYB * UXB, PC = B::PYB * PXB, RCS = TY * TX, SXW = G::SXW;
+  static_assert(DIST >= 2, "step k waits for plane k+1, issued at the end of step k+1-DIST");
+  extern __shared__ __align__(128) unsigned char smem[];
+  float(*sqx)[3][TY][SXW] = reinterpret_cast<float(*)[3][TY][SXW]>(smem + G::SQX_OFF);
+  float(*sqy)[3][TY + 2][TX] = reinterpret_cast<float(*)[3][TY + 2][TX]>(smem + G::SQY_OFF);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + G::BAR_OFF);
+
+  const Tile T = tiles[blockIdx.x];
+  const Desc& Dg = descs[T.desc];
+  const TMaps* M = maps + T.desc;
+  const int nz = Dg.nz, ny = Dg.ny, nx = Dg.nx;
+  const int cs = (int)Dg.cs;
+  const int plane = Dg.pitch * ny;
+  const int z0 = T.z0z1 & 0xffff, z1 = T.z0z1 >> 16;
+  const CUtensorMap* mu = &M->u[a.src];
+  const CUtensorMap* mp = &M->p[a.src];
+
+  const int tid = threadIdx.x;
+  int role, lx, ly;  // position relative to (x0, y0)
+  if (tid < G::NI) {
+    role = 0;
+    lx = V * (tid % G::PW);
+    ly = tid / G::PW;
+  } else if (tid < G::NI + G::NH) {
+    const int h = tid - G::NI;
+    role = 1;
+    lx = V * (h % G::PW);
+    ly = (h < G::PW) ? -1 : TY;
+  } else {
+    const int h = tid - G::NI - G::NH;
+    role = 2;
+    lx = (h < TY) ? -1 : TX;
+    ly = h % TY;
+  }
+  const int gx = T.x0 + lx, gy = T.y0 + ly;
+  const bool active = gx >= 0 && gx < nx && gy >= 0 && gy < ny;
+  const bool full = gx + V - 1 < nx;          // roles 0/1: every voxel of the lane is inside
+  const int uo = (ly + 2) * UXB + (lx + AU);  // own (first) voxel in a u box component
+  const int po = (ly + 1) * PXB + (lx + AP);  // own (first) voxel in a p/D box component
+  const int ro = ly * TX + lx;                // own voxels in an rc/gw box (role 0)
+  const long long col0 = (long long)gy * Dg.pitch + gx;
+  SU* __restrict__ u_dst = reinterpret_cast<SU*>(Dg.u[a.src ^ 1]) + col0;
+  SP* __restrict__ p_dst = reinterpret_cast<SP*>(Dg.p[a.src ^ 1]) + col0;
+  const int bdry = a.bdry;
+  Stencil3 fx[V], ax[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    fx[v] = fwd_coef(gx + v, nx, bdry, Dg.hx);
+    ax[v] = adj_coef(gx + v, nx, bdry, 1.0f / Dg.hx);
+  }
+  const Stencil3 fy = fwd_coef(gy, ny, bdry, Dg.hy);
+  const Stencil3 ay = adj_coef(gy, ny, bdry, 1.0f / Dg.hy);
+  const float ihz = 1.0f / Dg.hz, hz = Dg.hz;
+
+  const int kb = max(z0 - 1, 0), ke = min(z1, nz - 1);
+  const int pl = max(kb - 1, 0), ph = min(ke + 1, nz - 1);
+  auto issue = [&](int q) {
+    const int r = q - pl;
+    uint64_t* bar = bars + r % G::NB;
+    unsigned char* U = smem + G::U_OFF + (r % G::NU) * B::U_SLOT;
+    if (q < kb) {
+      mbar_arrive_expect_tx(bar, (uint32_t)B::U_TX);
+      tma_load_4d(U, mu, bar, T.x0 - AU, T.y0 - 2, q, 0);
+      return;
+    }
+    unsigned char* PD = smem + G::PD_OFF + ((q - kb) % G::NPD) * B::PD_SLOT;
+    unsigned char* R = smem + G::R_OFF + ((q - kb) % G::NR) * B::R_SLOT;
+    mbar_arrive_expect_tx(bar, (uint32_t)B::FULL_TX);
+    tma_load_4d(U, mu, bar, T.x0 - AU, T.y0 - 2, q, 0);
+    tma_load_4d(PD, mp, bar, T.x0 - AP, T.y0 - 1, q, 0);
+    tma_load_4d(PD + B::P_SLOT, &M->D, bar, T.x0 - AP, T.y0 - 1, q, 0);
+    tma_load_4d(R, &M->rc, bar, T.x0, T.y0, q, 0);
+    tma_load_4d(R + B::RC_SLOT, &M->gw, bar, T.x0, T.y0, q, 0);
+  };
+  auto ubox = [&](int q) {
+    return reinterpret_cast<const SU*>(smem + G::U_OFF + ((q - pl) % G::NU) * B::U_SLOT);
+  };
+  auto rbox = [&](int q) { return smem + G::R_OFF + ((q - kb) % G::NR) * B::R_SLOT; };
+
+  // q cells that no lane writes (outside the volume, the unused qx column x0+TX+1) are read
+  // with zero stencil coefficients: they must hold zeros (0 * NaN = NaN)
+  for (int i = tid; i < (G::SQX_BYTES + G::SQY_BYTES) / 4; i += blockDim.x)
+    reinterpret_cast<float*>(smem + G::SQX_OFF)[i] = 0.f;
+  if (tid == 0) {
+    for (int s = 0; s < G::NB; ++s) mbar_init(bars + s, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  int issued = pl - 1;
+  if (tid == 0) {
+    const int last = min(kb + DIST - 1, ph);
+    for (int q = pl; q <= last; ++q) issue(q);
+    issued = last;
+  }
+  int waited = pl - 1;
+  bool bad = false;
+
+  // q_z of the own voxels (role 0) at planes k-2, k-1, k
+  float qmm[V][3] = {}, qm[V][3] = {}, qc[V][3] = {};
+  const float wtv2 = a.wtv * a.wtv;
+
+  // x/y part of the divergence at plane j (q rows of slot j & 1), loaded before the dual
+  auto load_dxy = [&](int j, float (&dxy)[V][3]) {
+    const int ps = j & 1;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float* qx = &sqx[ps][c][ly][lx + 2];
+      float o[V], dn[V], up[V], oy[V];
+      Lane<V, float>::sh(qx, o);
+      const float L = qx[-1], R = qx[V];
+      Lane<V, float>::sh(&sqy[ps][c][ly][lx], dn);
+      Lane<V, float>::sh(&sqy[ps][c][ly + 2][lx], up);
+      if (GEN) Lane<V, float>::sh(&sqy[ps][c][ly + 1][lx], oy);
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const float prev = v == 0 ? L : o[v - 1], next = v == V - 1 ? R : o[v + 1];
+        const float dx = apply3<GEN>(ax[v], prev, GEN ? o[v] : 0.f, next);
+        dxy[v][c] = dx + apply3<GEN>(ay, dn[v], GEN ? oy[v] : 0.f, up[v]);
+      }
+    }
+  };
+  // primal of plane j: qn = q_z(j+1), uj = own u at plane j
+  auto finish_primal = [&](int j, const float (&dxy)[V][3], const float (&qn)[V][3], const float (&uj)[V][3]) {
+    const unsigned char* R = rbox(j);
+    const SP* RC = reinterpret_cast<const SP*>(R) + ro;
+    const SP* GW = reinterpret_cast<const SP*>(R + B::RC_SLOT) + ro;
+    const Stencil3 az = adj_coef(j, nz, bdry, ihz);
+    float rc[V], g[3][V], n[3][V];
+    Lane<V, SP>::sh(RC, rc);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) Lane<V, SP>::sh(GW + c * RCS, g[c]);
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      float d[3], gv[3], nv[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        d[c] = dxy[v][c] + apply3<GEN>(az, qmm[v][c], qm[v][c], qn[v][c]);
+        gv[c] = g[c][v];
+      }
+      primal_voxel(uj[v], d, a.tau, a.factor, rc[v], gv, nv);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) n[c][v] = nv[c];
+    }
+    SU* dst = u_dst + (long long)j * plane;
+    if (full) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) Lane<V, SU>::st(dst + c * cs, n[c]);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) Store<SU>::st(dst + c * cs, n[c][0]);
+    }
+  };
+
+  // One plane step; WITH_PRIMAL: role 0 also finishes plane k-1.
+  auto step = [&](const int k, auto with_primal) {
+    constexpr bool WP = decltype(with_primal)::value;
+    const int need = min(k + 1, ph);
+    while (waited < need && !bad) {
+      ++waited;
+      const int r = waited - pl;
+      if (!mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1))) bad = true;
+    }
+    const int qs = k & 1;
+    const SU* Uk = ubox(k) + uo;
+    const unsigned char* PD = smem + G::PD_OFF + ((k - kb) % G::NPD) * B::PD_SLOT;
+    const Stencil3 fz = fwd_coef(k, nz, bdry, hz);
+    const bool has_m = k - 1 >= pl, has_p = k + 1 <= ph;
+    const SU* Um = ubox(has_m ? k - 1 : k) + uo;
+    const SU* Up = ubox(has_p ? k + 1 : k) + uo;
+    if (role != 2) {
+      if (active && !bad) {
+        float dxy[V][3];
+        if (WP && role == 0) load_dxy(k - 1, dxy);
+        // own voxels at planes k-1, k, k+1
+        float um[V][3], uc[V][3], up[V][3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          float m[V], o[V], n[V];
+          Lane<V, SU>::sh(Um + c * UC, m);
+          Lane<V, SU>::sh(Uk + c * UC, o);
+          Lane<V, SU>::sh(Up + c * UC, n);
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            um[v][c] = has_m ? m[v] : 0.f;
+            uc[v][c] = o[v];
+            up[v][c] = has_p ? n[v] : 0.f;
+          }
+        }
+        const SP* P = reinterpret_cast<const SP*>(PD) + po;
+        const SP* Dm = reinterpret_cast<const SP*>(PD + B::P_SLOT) + po;
+        float pv[9][V], Dv[6][V];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) Lane<V, SP>::sh(P + c * PC, pv[c]);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) Lane<V, SP>::sh(Dm + c * PC, Dv[c]);
+        float pk[V][9], Dk[V][6];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+#pragma unroll
+          for (int c = 0; c < 9; ++c) pk[v][c] = pv[c][v];
+#pragma unroll
+          for (int c = 0; c < 6; ++c) Dk[v][c] = Dv[c][v];
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const SU* u = Uk + c * UC;
+          const float L = Store<SU>::sh(u - 1), R = Store<SU>::sh(u + V);
+          float dn[V], upy[V];
+          Lane<V, SU>::sh(u - UXB, dn);
+          Lane<V, SU>::sh(u + UXB, upy);
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            const float prev = v == 0 ? L : uc[v - 1][c], next = v == V - 1 ? R : uc[v + 1][c];
+            const float ex = apply3<GEN>(fx[v], prev, uc[v][c], next);
+            const float ey = apply3<GEN>(fy, dn[v], uc[v][c], upy[v]);
+            const float ez = apply3<GEN>(fz, um[v][c], uc[v][c], up[v][c]);
+            dual_row(Dk[v], ex, ey, ez, pk[v][3 * c], pk[v][3 * c + 1], pk[v][3 * c + 2], a.sigma, a.wtv, wtv2);
+          }
+        }
+        if (role == 0) {
+          if (k >= z0 && k < z1) {
+            SP* dst = p_dst + (long long)k * plane;
+            if (full) {
+#pragma unroll
+              for (int c = 0; c < 9; ++c) {
+                float t[V];
+#pragma unroll
+                for (int v = 0; v < V; ++v) t[v] = pk[v][c];
+                Lane<V, SP>::st(dst + c * cs, t);
+              }
+            } else {
+#pragma unroll
+              for (int c = 0; c < 9; ++c) Store<SP>::st(dst + c * cs, pk[0][c]);
+            }
+          }
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            float qx[V], qy[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              const float* D = Dk[v];
+              const float* p = &pk[v][3 * c];
+              qx[v] = D[0] * p[0] + D[1] * p[1] + D[2] * p[2];
+              qy[v] = D[1] * p[0] + D[3] * p[1] + D[4] * p[2];
+              qc[v][c] = D[2] * p[0] + D[4] * p[1] + D[5] * p[2];
+            }
+            Lane<V, float>::st(&sqx[qs][c][ly][lx + 2], qx);
+            Lane<V, float>::st(&sqy[qs][c][ly + 1][lx], qy);
+          }
+          if (WP) finish_primal(k - 1, dxy, qc, um);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            float qy[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              const float* D = Dk[v];
+              const float* p = &pk[v][3 * c];
+              qy[v] = D[1] * p[0] + D[3] * p[1] + D[4] * p[2];
+            }
+            Lane<V, float>::st(&sqy[qs][c][ly + 1][lx], qy);
+          }
+        }
+      }
+    } else if (active && !bad) {
+      // halo column: one voxel
+      const SP* P = reinterpret_cast<const SP*>(PD) + po;
+      const SP* Dm = reinterpret_cast<const SP*>(PD + B::P_SLOT) + po;
+      float pk[9], Dk[6];
+#pragma unroll
+      for (int c = 0; c < 9; ++c) pk[c] = Store<SP>::sh(P + c * PC);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) Dk[c] = Store<SP>::sh(Dm + c * PC);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const SU* u = Uk + c * UC;
+        const float o = Store<SU>::sh(u);
+        const float m = has_m ? Store<SU>::sh(Um + c * UC) : 0.f;
+        const float n = has_p ? Store<SU>::sh(Up + c * UC) : 0.f;
+        const float ex = apply3<GEN>(fx[0], Store<SU>::sh(u - 1), o, Store<SU>::sh(u + 1));
+        const float ey = apply3<GEN>(fy, Store<SU>::sh(u - UXB), o, Store<SU>::sh(u + UXB));
+        const float ez = apply3<GEN>(fz, m, o, n);
+        dual_row(Dk, ex, ey, ez, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2], a.sigma, a.wtv, wtv2);
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        sqx[qs][c][ly][lx + 2] = Dk[0] * pk[3 * c] + Dk[1] * pk[3 * c + 1] + Dk[2] * pk[3 * c + 2];
+    }
+    // everyone is done with plane k's p/D, plane k-1's u and rc/gw, and q rows of plane k-1
+    if (__syncthreads_or(bad)) {
+      bad = true;
+      return;
+    }
+    if (tid == 0 && k + DIST <= ph && k + DIST > issued) {
+      issue(k + DIST);
+      issued = k + DIST;
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        qmm[v][c] = qm[v][c];
+        qm[v][c] = qc[v][c];
+      }
+  };
+
+  // the first one or two steps have no finished plane (j = k-1 < z0)
+  const int kp = min(z0 + 1, ke + 1);
+  int k = kb;
+  for (; k < kp && !bad; ++k) step(k, std::false_type{});
+  for (; k <= ke && !bad; ++k) step(k, std::true_type{});
+  if (bad) {
+    if (tid == 0) {
+      atomicOr(status, SVS_DEV_TIMEOUT);
+      // wait (bounded) for the copies this CTA still has in flight before it exits
+      for (int q = max(waited + 1, pl); q <= issued; ++q) {
+        const int r = q - pl;
+        mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1));
+      }
+    }
+    return;
+  }
+  if (z1 >= nz) {
+    const int j = nz - 1;
+    if (role == 0 && active && j >= z0) {
+      float dxy[V][3], uj[V][3];
+      const float zero[V][3] = {};
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float o[V];
+        Lane<V, SU>::sh(ubox(j) + uo + c * UC, o);
+#pragma unroll
+        for (int v = 0; v < V; ++v) uj[v][c] = o[v];
+      }
+      load_dxy(j, dxy);
+      finish_primal(j, dxy, zero, uj);
+    }
+  }
+}
+
+// Compiled shapes of the split-role form (tile, prefetch distance, voxels per lane, CTAs per SM
+// the register budget is sized for); instantiated in svs_split.cu.
+struct SplitShape {
+  int tx, ty, dist, v, minb;
+};
+constexpr SplitShape kSplitShapes[] = {
+    {32, 8, 3, 2, 1},  {32, 8, 4, 2, 1}, {16, 16, 3, 2, 1}, {40, 8, 3, 2, 2}, {32, 16, 3, 2, 1},
+    {40, 16, 3, 2, 1}, {32, 8, 3, 1, 2}, {32, 8, 4, 1, 2},  {16, 16, 3, 1, 2}, {32, 16, 2, 1, 1},
+    {32, 16, 3, 1, 1}, {40, 8, 3, 1, 2}};
+constexpr int kNumSplitShapes = sizeof(kSplitShapes) / sizeof(kSplitShapes[0]);
+
+// Split-role variant `idx` for a storage mode. op 0: set the kernels' shared-memory attribute
+// and return the TMA box shapes {u x, u y, p x, p y} in `box` (false if the variant does not
+// fit); op 1: launch one iteration over `ntiles` tiles on stream s.
+bool split_variant(int storage, int idx, int op, bool gen, unsigned ntiles, const Tile* tiles, const Desc* descs,
+                   const TMaps* maps, const IterArgs* a, int* status, cudaStream_t s, int* box);
 
 }  // namespace svs

@@ -36,11 +36,27 @@ namespace svs {
 namespace {
 
 // Iterate-kernel variants compiled into the library (id 1..N; 0 = automatic).
+enum TileForm { kPlain = 0, kTma = 1, kSplit = 2 };
 struct TileShape {
-  int tx, ty, dist;  // dist = 0: plain-load form; > 0: TMA form with that prefetch distance
+  int tx, ty, dist;  // dist: TMA prefetch distance in planes (0 for the plain-load form)
+  int form;
+  int split;         // index into kSplitShapes (split-role form)
 };
-constexpr TileShape kTileShapes[] = {{32, 8, 2}, {32, 8, 3}, {64, 4, 2}, {16, 16, 2}, {32, 16, 2},
-                                     {32, 8, 0}, {32, 4, 0}, {16, 16, 0}};
+constexpr TileShape split_entry(int i) {
+  return {kSplitShapes[i].tx, kSplitShapes[i].ty, kSplitShapes[i].dist, kSplit, i};
+}
+constexpr TileShape kTileShapes[] = {
+    {32, 8, 2, kTma, 0},   {32, 8, 3, kTma, 0},   {64, 4, 2, kTma, 0},   {16, 16, 2, kTma, 0},
+    {32, 16, 2, kTma, 0},  {32, 8, 0, kPlain, 0}, {32, 4, 0, kPlain, 0}, {16, 16, 0, kPlain, 0},
+    split_entry(0),        split_entry(1),        split_entry(2),        split_entry(3),
+    split_entry(4),        split_entry(5),        split_entry(6),        split_entry(7),
+    split_entry(8),        split_entry(9),        split_entry(10),       split_entry(11)};
+constexpr bool split_table_complete() {
+  int n = 0;
+  for (const TileShape& t : kTileShapes) n += t.form == kSplit;
+  return n == kNumSplitShapes;
+}
+static_assert(split_table_complete(), "every compiled split-role shape has a variant id");
 constexpr int kNumTileShapes = sizeof(kTileShapes) / sizeof(kTileShapes[0]);
 
 // ------------------------------------------------------------------------------ small kernels
@@ -422,21 +438,23 @@ bool encode_field(CUtensorMap* m, int es_bytes, bool bf16, const void* base, con
   return r == CUDA_SUCCESS;
 }
 
-template <typename SU, typename SP, int TX, int TY, int DIST>
-bool encode_maps(svs_plan& P, std::vector<TMaps>& maps, int level) {
-  using G = TmaGeom<SU, SP, TX, TY, DIST>;
+// Tensor maps of every pair of a level, boxes {ux, uy} for u, {px, py} for p and D, tile {tx, ty}
+// for rc and gw.
+bool encode_maps(svs_plan& P, std::vector<TMaps>& maps, int level, int ux, int uy, int px, int py, int tx,
+                 int ty) {
   const bool bf = is_bf16(P.prm.storage);
+  const int esu = (int)flow_bytes(P.prm.storage), esp = (int)field_bytes(P.prm.storage);
   for (int i = 0; i < P.num_pairs; ++i) {
     const size_t k = (size_t)level * P.num_pairs + i;
     const Desc& d = P.h_descs[k];
     TMaps& m = maps[k];
-    bool ok = encode_field(&m.u[0], G::ESU, bf, d.u[0], d, 3, G::UXB, G::UYB) &&
-              encode_field(&m.u[1], G::ESU, bf, d.u[1], d, 3, G::UXB, G::UYB) &&
-              encode_field(&m.p[0], G::ESP, bf, d.p[0], d, 9, G::PXB, G::PYB) &&
-              encode_field(&m.p[1], G::ESP, bf, d.p[1], d, 9, G::PXB, G::PYB) &&
-              encode_field(&m.D, G::ESP, bf, d.D, d, 6, G::PXB, G::PYB) &&
-              encode_field(&m.rc, G::ESP, bf, d.rc, d, 1, TX, TY) &&
-              encode_field(&m.gw, G::ESP, bf, d.gw, d, 3, TX, TY);
+    bool ok = encode_field(&m.u[0], esu, bf, d.u[0], d, 3, ux, uy) &&
+              encode_field(&m.u[1], esu, bf, d.u[1], d, 3, ux, uy) &&
+              encode_field(&m.p[0], esp, bf, d.p[0], d, 9, px, py) &&
+              encode_field(&m.p[1], esp, bf, d.p[1], d, 9, px, py) &&
+              encode_field(&m.D, esp, bf, d.D, d, 6, px, py) &&
+              encode_field(&m.rc, esp, bf, d.rc, d, 1, tx, ty) &&
+              encode_field(&m.gw, esp, bf, d.gw, d, 3, tx, ty);
     if (!ok) return false;
   }
   return true;
@@ -453,7 +471,7 @@ bool tma_prepare(svs_plan& P, std::vector<TMaps>& maps, int level) {
     cudaGetLastError();
     return false;
   }
-  return encode_maps<SU, SP, TX, TY, DIST>(P, maps, level);
+  return encode_maps(P, maps, level, G::UXB, G::UYB, G::PXB, G::PYB, TX, TY);
 }
 
 // Dispatch over the compiled variants. `op` 0: prepare (attributes + maps), 1: launch.
@@ -498,6 +516,16 @@ bool iter_variant(svs_plan& P, std::vector<TMaps>* maps, int level, int tid, int
 
 bool iter_dispatch(svs_plan& P, std::vector<TMaps>* maps, int level, int tid, int op, const IterArgs* a,
                    cudaStream_t s) {
+  const TileShape& ts = kTileShapes[tid - 1];
+  if (ts.form == kSplit) {
+    const unsigned nt = (unsigned)P.h_tiles[level].size();
+    const Tile* tl = P.d_tiles.empty() ? nullptr : P.d_tiles[level];
+    const bool gen = P.prm.boundary != SVS_BOUNDARY_MIRROR;
+    int box[4] = {0, 0, 0, 0};
+    if (!split_variant(P.prm.storage, ts.split, op, gen, nt, tl, P.d_descs, P.d_maps, a, P.d_status, s, box))
+      return false;
+    return op != 0 || encode_maps(P, *maps, level, box[0], box[1], box[2], box[3], ts.tx, ts.ty);
+  }
   switch (P.prm.storage) {
     case SVS_STORAGE_BF16: return iter_variant<__nv_bfloat16, __nv_bfloat16>(P, maps, level, tid, op, a, s);
     case SVS_STORAGE_F16: return iter_variant<__half, __half>(P, maps, level, tid, op, a, s);
@@ -507,10 +535,21 @@ bool iter_dispatch(svs_plan& P, std::vector<TMaps>* maps, int level, int tid, in
   }
 }
 
-// Automatic choice (measured on B200 with 80^3 batches): 32x8 tiles, prefetch distance 2 for
-// 4-byte fields (two CTAs per SM fit), 3 for 2-byte fields; the plain-load 32x8 form if TMA
+constexpr int split_id(int tx, int ty, int dist, int v) {
+  for (int i = 0; i < kNumTileShapes; ++i)
+    if (kTileShapes[i].form == kSplit && kTileShapes[i].tx == tx && kTileShapes[i].ty == ty &&
+        kTileShapes[i].dist == dist && kSplitShapes[kTileShapes[i].split].v == v)
+      return i + 1;
+  return 0;
+}
+constexpr int kAutoF32 = split_id(32, 16, 3, 2), kAuto16 = split_id(16, 16, 3, 1);
+static_assert(kAutoF32 > 0 && kAuto16 > 0, "automatic variants are compiled");
+
+// Automatic choice (measured on B200 with 80^3 batches): split-role pipelines with prefetch
+// distance 3, 32x16 tiles of voxel pairs when the fields are 4-byte (one CTA per SM) and 16x16
+// tiles of single voxels when they are 2-byte (two CTAs per SM); the plain-load 32x8 form if TMA
 // descriptors cannot be built.
-int auto_tile(const svs_plan& P) { return P.prm.storage == SVS_STORAGE_F32 ? 1 : 2; }
+int auto_tile(const svs_plan& P) { return P.prm.storage == SVS_STORAGE_F32 ? kAutoF32 : kAuto16; }
 
 void build_tiles(svs_plan& P, int level, int tid) {
   const TileShape ts = kTileShapes[tid - 1];
@@ -662,6 +701,17 @@ using namespace svs;
 extern "C" {
 
 int svs_tvl1_num_tiles(void) { return kNumTileShapes; }
+
+svs_status svs_tvl1_tile_info(int tile_id, int* tx, int* ty, int* dist, int* form, int* lane_voxels) {
+  SVS_REQUIRE(tile_id >= 1 && tile_id <= kNumTileShapes, "svs_tvl1_tile_info: unknown tile id");
+  const TileShape& t = kTileShapes[tile_id - 1];
+  if (tx) *tx = t.tx;
+  if (ty) *ty = t.ty;
+  if (dist) *dist = t.dist;
+  if (form) *form = t.form;
+  if (lane_voxels) *lane_voxels = t.form == kSplit ? kSplitShapes[t.split].v : 1;
+  return SVS_OK;
+}
 
 svs_status svs_tvl1_plan_create(const svs_tvl1_params* prm, int num_pairs, const int* dims,
                                 svs_plan** out) {

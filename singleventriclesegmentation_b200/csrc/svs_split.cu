@@ -1,0 +1,62 @@
+// Instantiations and launch of the split-role iterate kernel (svs_iterate.cuh) for every storage
+// mode and compiled shape, in a translation unit of their own so that they compile in parallel
+// with the rest of the library.
+#include "svs_iterate.cuh"
+
+namespace svs {
+namespace {
+
+template <typename SU, typename SP, int I>
+bool run(int op, bool gen, unsigned nt, const Tile* tiles, const Desc* descs, const TMaps* maps,
+         const IterArgs* a, int* status, cudaStream_t s, int* box) {
+  constexpr SplitShape S = kSplitShapes[I];
+  using G = SplitGeom<SU, SP, S.tx, S.ty, S.dist, S.v>;
+  auto* kf = iterate_split_kernel<SU, SP, S.tx, S.ty, S.dist, S.v, S.minb, false>;
+  auto* kt = iterate_split_kernel<SU, SP, S.tx, S.ty, S.dist, S.v, S.minb, true>;
+  if (op == 0) {
+    if (G::SMEM > 227 * 1024) return false;
+    if (cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM) != cudaSuccess ||
+        cudaFuncSetAttribute(kt, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    box[0] = G::B::UXB;
+    box[1] = G::B::UYB;
+    box[2] = G::B::PXB;
+    box[3] = G::B::PYB;
+    return true;
+  }
+  (gen ? kt : kf)<<<nt, G::NT, G::SMEM, s>>>(tiles, descs, maps, *a, status);
+  return true;
+}
+
+template <typename SU, typename SP>
+bool dispatch(int idx, int op, bool gen, unsigned nt, const Tile* tiles, const Desc* descs, const TMaps* maps,
+              const IterArgs* a, int* status, cudaStream_t s, int* box) {
+#define SVS_SPLIT(I) \
+  case I: return run<SU, SP, I>(op, gen, nt, tiles, descs, maps, a, status, s, box);
+  static_assert(kNumSplitShapes == 12, "one case per compiled shape");
+  switch (idx) {
+    SVS_SPLIT(0) SVS_SPLIT(1) SVS_SPLIT(2) SVS_SPLIT(3) SVS_SPLIT(4) SVS_SPLIT(5)
+    SVS_SPLIT(6) SVS_SPLIT(7) SVS_SPLIT(8) SVS_SPLIT(9) SVS_SPLIT(10) SVS_SPLIT(11)
+    default: return false;
+  }
+#undef SVS_SPLIT
+}
+
+}  // namespace
+
+bool split_variant(int storage, int idx, int op, bool gen, unsigned nt, const Tile* tiles, const Desc* descs,
+                   const TMaps* maps, const IterArgs* a, int* status, cudaStream_t s, int* box) {
+  switch (storage) {
+    case SVS_STORAGE_BF16:
+      return dispatch<__nv_bfloat16, __nv_bfloat16>(idx, op, gen, nt, tiles, descs, maps, a, status, s, box);
+    case SVS_STORAGE_F16: return dispatch<__half, __half>(idx, op, gen, nt, tiles, descs, maps, a, status, s, box);
+    case SVS_STORAGE_BF16_FLOW32:
+      return dispatch<float, __nv_bfloat16>(idx, op, gen, nt, tiles, descs, maps, a, status, s, box);
+    case SVS_STORAGE_F16_FLOW32: return dispatch<float, __half>(idx, op, gen, nt, tiles, descs, maps, a, status, s, box);
+    default: return dispatch<float, float>(idx, op, gen, nt, tiles, descs, maps, a, status, s, box);
+  }
+}
+
+}  // namespace svs

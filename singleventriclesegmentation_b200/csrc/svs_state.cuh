@@ -29,6 +29,32 @@ template <> struct Store<__half> {
   static __device__ __forceinline__ void st(__half* p, float v) { *p = __float2half_rn(v); }
 };
 
+// Two x-adjacent values (an even element index, so 8- or 4-byte aligned) as one access; the
+// roundings are those of Store<S> applied to each value.
+template <typename S> struct Pair;
+template <> struct Pair<float> {
+  static __device__ __forceinline__ float2 sh(const float* p) { return *reinterpret_cast<const float2*>(p); }
+  static __device__ __forceinline__ void st(float* p, float a, float b) {
+    *reinterpret_cast<float2*>(p) = make_float2(a, b);
+  }
+};
+template <> struct Pair<__nv_bfloat16> {
+  static __device__ __forceinline__ float2 sh(const __nv_bfloat16* p) {
+    return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+  }
+  static __device__ __forceinline__ void st(__nv_bfloat16* p, float a, float b) {
+    *reinterpret_cast<__nv_bfloat162*>(p) = __floats2bfloat162_rn(a, b);
+  }
+};
+template <> struct Pair<__half> {
+  static __device__ __forceinline__ float2 sh(const __half* p) {
+    return __half22float2(*reinterpret_cast<const __half2*>(p));
+  }
+  static __device__ __forceinline__ void st(__half* p, float a, float b) {
+    *reinterpret_cast<__half2*>(p) = __floats2half2_rn(a, b);
+  }
+};
+
 // One (pair, level) of the batch.
 // Float fields (I0, I1, g1 planes) are dense [nz][ny][nx]. Iteration-state fields of storage
 // type S (D, rc, gw, u[2], p[2]) are planar and PITCHED: component c of voxel (z, y, x) is at

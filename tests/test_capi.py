@@ -51,3 +51,19 @@ def test_plan_rejects_too_small_pyramids():
     h = ctypes.c_void_p()
     st = _lib.lib().svs_tvl1_plan_create(ctypes.byref(p), 1, dims, ctypes.byref(h))
     assert st == 1 and b"at least 3 nodes" in _lib.lib().svs_last_error()
+
+
+def test_tile_info_lists_every_variant():
+    n = _lib.lib().svs_tvl1_num_tiles()
+    infos = [_lib.tile_info(t) for t in range(1, n + 1)]
+    assert {i["form"] for i in infos} == {"plain", "tma", "split"}
+    for i in infos:
+        assert i["tx"] % 8 == 0 and i["ty"] > 0  # tile origins keep TMA boxes 16-byte aligned
+        assert (i["dist"] == 0) == (i["form"] == "plain")
+        if i["form"] == "split":
+            assert i["lane_voxels"] in (1, 2) and i["dist"] >= 2
+            assert (i["tx"] // i["lane_voxels"] * i["ty"]) % 32 == 0  # interior lanes fill whole warps
+    import pytest
+    for bad in (0, n + 1):
+        with pytest.raises(_lib.SVSError):
+            _lib.tile_info(bad)

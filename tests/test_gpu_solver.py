@@ -121,13 +121,22 @@ def test_batch_invariance_and_uneven_sizes(cuda):
         assert torch.equal(ua, ub)
 
 
-@pytest.mark.parametrize("storage", ["f32", "bf16", "bf16-flow32"])
-def test_tile_variants_agree(cuda, pair24, storage):
-    """Every iterate-kernel variant (TMA pipelines and plain-load forms, all tile shapes) gives
-    the same result: bitwise within a family, to rounding across the two families."""
+@pytest.mark.parametrize("storage,shape,over", [
+    ("f32", (24, 24, 24), {}),
+    ("bf16", (24, 24, 24), {}),
+    ("bf16-flow32", (24, 24, 24), {}),
+    # odd widths (a last pair of voxels with one outside the volume), two tiles in x and y
+    ("f16-flow32", (21, 37, 45), {}),
+    ("f32", (21, 37, 45), {"boundary_type": "NEAREST"}),
+])
+def test_tile_variants_agree(cuda, storage, shape, over):
+    """Every iterate-kernel variant (TMA pipelines, split-role TMA pipelines and plain-load forms,
+    all tile shapes) gives the same result: bitwise among the TMA and split-role forms (the same
+    expression sequence per voxel), bitwise among the plain-load forms, and to rounding across
+    the two."""
     from singleventriclesegmentation_b200 import _lib
-    I0, I1, _ = pair24
-    solver, _ = make_solver(storage=storage, max_warps=2, max_outer_iterations=30)
+    I0, I1, _ = synthetic.frame_pair(shape, seed=11)
+    solver, _ = make_solver(storage=storage, max_warps=2, max_outer_iterations=30, **over)
     res = {}
     for tid in range(1, _lib.lib().svs_tvl1_num_tiles() + 1):
         solver.tile_id = tid
@@ -139,9 +148,10 @@ def test_tile_variants_agree(cuda, pair24, storage):
             continue
         for plan in solver._plans.values():
             plan.check()
-    tma = [t for t in res if t <= 5]
-    plain = [t for t in res if t >= 6]
-    assert tma and plain
+    forms = {t: _lib.tile_info(t)["form"] for t in res}
+    tma = [t for t in res if forms[t] in ("tma", "split")]
+    plain = [t for t in res if forms[t] == "plain"]
+    assert tma and plain and any(forms[t] == "split" for t in tma)
     for fam in (tma, plain):
         for t in fam[1:]:
             assert torch.equal(res[t], res[fam[0]]), (t, fam[0])
