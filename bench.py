@@ -8,6 +8,15 @@ flows. The sequence stands in for the reference's 80^3 x 35-frame cine MRI data.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--storage f16-flow32|f32|...] [--impl reference]
 
+Before warm-up the iterate-kernel variant of each pyramid level is autotuned on the plan's own
+state. Beside the headline line's contract keys it reports the plain GPU form (the reference's
+per-operator structure on this package's kernels, one 80^3 pair, full schedule) for the ratio the
+metric asks for. Further workloads, one JSON line each, on one GPU:
+
+    python bench.py --workload uneven    # 64 pairs, dims per axis on {40, ..., 128}
+    python bench.py --workload mixed     # the sequence + 16 x 128^3, 16-bit storage modes, EPE vs FP64 oracle
+    python bench.py --workload serving   # Poisson request streams through the continuous-batching server
+
 Multi-GPU: one process per GPU (torchrun); every rank solves its own sequence (replicas, weak
 scaling, no collective on the data path); NCCL is used only for the barrier and the max-over-ranks
 timing. Rank 0 prints one JSON line.
@@ -44,7 +53,15 @@ def parse():
     ap.add_argument("--storage", default="f16-flow32", choices=["f32", "bf16", "f16", "bf16-flow32", "f16-flow32"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain-form", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--frames", type=int, default=T_FRAMES)
+    ap.add_argument("--workload", default="sequence", choices=["sequence", "uneven", "mixed", "serving"],
+                    help="sequence: 35-frame 80^3 cine sequence (the headline line); uneven: 64 pairs of "
+                         "mixed sizes; mixed: the sequence plus 16 pairs of 128^3 with EPE against the FP64 "
+                         "oracle; serving: Poisson request stream through the continuous-batching server")
+    ap.add_argument("--rates", default="0.1,1,10,50", help="serving: arrival rates (requests/s)")
+    ap.add_argument("--requests", type=int, default=6, help="serving: requests per rate")
     return ap.parse_args()
 
 
@@ -192,11 +209,238 @@ def config_dict(args, storage):
             "parallelism": f"replicas x{args.gpus}"}
 
 
+# ------------------------------------------------------------------------ shared helpers
+def tune_plan(plan, storage: str, levels: int = 3):
+    """Pick the fastest iterate-kernel variant per pyramid level on the plan's own state
+    (TMA and split-role forms)."""
+    from singleventriclesegmentation_b200 import _lib, autotune
+    n = int(_lib.lib().svs_tvl1_num_tiles())
+    cands = [t for t in range(1, n + 1) if _lib.tile_info(t)["form"] != "plain"]
+    return autotune.tune(plan, storage, levels, candidates=cands, use_cache=False, iters=6)
+
+
+def iterate_roofline(plan, storage: str, level_voxels: int, stream, dev):
+    """The dominant kernel (fused iteration, level 0) timed alone on the live state with CUDA
+    events: (ms per launch, algorithmic bytes per launch)."""
+    import torch
+    n_it = 30
+    plan.bench_iterations(0, 3)
+    torch.cuda.synchronize(dev)
+    e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e4.record(stream)
+    plan.bench_iterations(0, n_it)
+    e5.record(stream)
+    torch.cuda.synchronize(dev)
+    it_ms = e4.elapsed_time(e5) / n_it
+    # bytes per voxel-iteration: read u 3, p 9, D 6, rc 1, gw 3; write u 3, p 9
+    ub = 2 if storage in ("bf16", "f16") else 4
+    fb = 4 if storage == "f32" else 2
+    return it_ms, level_voxels * (6 * ub + 28 * fb)
+
+
+def plain_form_rate(dev, seq_dev):
+    """The plain GPU form (the reference's per-operator structure, tvl13d.py:122-255, on this
+    package's per-operator kernels, FP32) on one 80^3 pair of the sequence with the full
+    schedule: pairs/s, timed with CUDA events."""
+    import torch
+    from singleventriclesegmentation_b200.tvl13d import TVL13DOpticalFlow
+    s = TVL13DOpticalFlow(3, 15, 300, 1.0, 0.025, 2, (0.5, 0.5, 0.25, 1.0), True, (5.0, 0.5), True, 1.0,
+                          "CUBIC_HERMITESPLINE", "MIRROR", "numDofs", (1, 1, 1), dev)
+    I0, I1 = seq_dev[1], seq_dev[0]
+    z = lambda: (torch.zeros(SHAPE + (3,), device=dev), torch.zeros(SHAPE + (3, 3), device=dev))
+    warm = TVL13DOpticalFlow(3, 1, 3, 1.0, 0.025, 2, (0.5, 0.5, 0.25, 1.0), True, (5.0, 0.5), True, 1.0,
+                             "CUBIC_HERMITESPLINE", "MIRROR", "numDofs", (1, 1, 1), dev)
+    warm.compute_unfused(I0, I1, *z())
+    torch.cuda.synchronize(dev)
+    u, p = z()
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    s.compute_unfused(I0, I1, u, p)
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    sec = e0.elapsed_time(e1) / 1000.0
+    return {"value": 1.0 / sec, "unit": "pairs/s", "seconds_per_pair": sec,
+            "form": "TVL13DOpticalFlow.compute_unfused: per-operator kernels, FP32, one 80^3 pair, full "
+                    "3 x 15 x 300 schedule"}
+
+
+# ----------------------------------------------------------------- further workloads (1 GPU)
+def _solver(dev, storage):
+    from singleventriclesegmentation_b200.tvl13d import TVL13DOpticalFlow
+    return TVL13DOpticalFlow(3, 15, 300, 1.0, 0.025, 2, (0.5, 0.5, 0.25, 1.0), True, (5.0, 0.5), True, 1.0,
+                             "CUBIC_HERMITESPLINE", "MIRROR", "numDofs", (1, 1, 1), dev, storage=storage)
+
+
+def _timed_solves(plan, I0s, I1s, outs, steps, warmup, dev):
+    import torch
+    for _ in range(warmup):
+        plan.solve(I0s, I1s, outs)
+    torch.cuda.synchronize(dev)
+    st = torch.cuda.current_stream(dev)
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        plan.solve(I0s, I1s, outs)
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    info = clocks.stop()
+    plan.check()
+    return e0.elapsed_time(e1) / steps, info
+
+
+def run_uneven(args):
+    """64 frame pairs with volume dims drawn per axis from {40, 48, ..., 128}, blob and sine
+    displacement recipe scaled to each volume, all in one batched solve (one CUDA graph), iterate
+    variants autotuned per level."""
+    import torch
+    from singleventriclesegmentation_b200 import synthetic
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    rng = np.random.default_rng(3)
+    dims = [tuple(int(v) for v in rng.choice(np.arange(40, 129, 8), size=3)) for _ in range(64)]
+    I0s, I1s = [], []
+    for i, d in enumerate(dims):
+        a, b, _ = synthetic.frame_pair(d, seed=100 + i, device="cuda")
+        I0s.append(torch.from_numpy(a).to(dev))
+        I1s.append(torch.from_numpy(b).to(dev))
+    outs = [torch.empty(d + (3,), device=dev) for d in dims]
+    solver = _solver(dev, args.storage)
+    plan = solver.plan_for(dims)
+    tiles = None if args.no_autotune else tune_plan(plan, args.storage)
+    ms, clocks = _timed_solves(plan, I0s, I1s, outs, args.steps, args.warmup, dev)
+    vox = sum(int(np.prod(d)) for d in dims)
+    it_ms, alg = iterate_roofline(plan, args.storage, vox, torch.cuda.current_stream(dev), dev)
+    peak, kind = measured_peaks()
+    print(json.dumps({
+        "metric": "uneven-size TV-L1 flow pairs/s", "value": len(dims) / (ms / 1000.0), "unit": "pairs/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "equivalent_80cube_pairs_per_s": vox / 512000.0 / (ms / 1000.0),
+        "dtype": f"f32 math, {args.storage} storage", "data": "synthetic",
+        "config": {"workload": "64 pairs, dims per axis uniform on {40,48,...,128} (seed 3), one batched solve",
+                   "total_voxels": vox, "storage": args.storage, "level_tiles": plan.level_tiles()[:3]},
+        "roofline": {"bound": "hbm", "achieved": alg / (it_ms / 1000.0) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / (it_ms / 1000.0) / 1e9 / peak, "peak_kind": kind, "launch_ms": it_ms},
+        "clocks": clocks}), flush=True)
+
+
+def run_mixed(args):
+    """The 35-frame 80^3 sequence (68 pairs) plus 16 pairs of 128^3 in one batched solve, in the
+    16-bit storage modes; end-point error against the FP64 oracle on a subset (two 80^3 pairs and
+    one 128^3 pair, the oracle run on the host) and Dice of the mask warped with each flow."""
+    import torch
+    from oracle import oracle as o
+    from singleventriclesegmentation_b200 import synthetic
+    from singleventriclesegmentation_b200.warping import Warp, dice
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    T = T_FRAMES
+    seq = torch.from_numpy(synthetic.cine_sequence(T=T, shape=SHAPE, seed=0, device="cuda")).to(dev)
+    pairs = synthetic.sequence_pairs(T, "forward") + synthetic.sequence_pairs(T, "backward")
+    I0s = [seq[a] for a, b in pairs]
+    I1s = [seq[b] for a, b in pairs]
+    big = [synthetic.frame_pair((128, 128, 128), seed=200 + i, device="cuda") for i in range(16)]
+    I0s += [torch.from_numpy(a).to(dev) for a, b, _ in big]
+    I1s += [torch.from_numpy(b).to(dev) for a, b, _ in big]
+    dims = [tuple(t.shape) for t in I0s]
+    subset = [0, len(pairs) - 1, len(pairs)]  # a forward and a backward 80^3 pair, one 128^3 pair
+    o.build()
+    o.set_threads(os.cpu_count() or 1)
+    P = o.SolverParams()
+    ref = {i: o.tvl1_compute(I0s[i].cpu().numpy(), I1s[i].cpu().numpy(), P, dtype=np.float64)[0] for i in subset}
+    warp = Warp("CUBIC_HERMITESPLINE", "MIRROR", "numDofs", (1, 1, 1))
+    out = []
+    for storage in ["bf16", "f16", "bf16-flow32", "f16-flow32"]:
+        outs = [torch.empty(d + (3,), device=dev) for d in dims]
+        solver = _solver(dev, storage)
+        plan = solver.plan_for(dims)
+        if not args.no_autotune:
+            tune_plan(plan, storage)
+        ms, clocks = _timed_solves(plan, I0s, I1s, outs, args.steps, args.warmup, dev)
+        epe, dices = {}, {}
+        for i in subset:
+            u = outs[i].cpu().numpy().astype(np.float64)
+            e = np.sqrt(((u - ref[i]) ** 2).sum(-1))
+            key = "x".join(map(str, dims[i])) + f"#{i}"
+            epe[key] = {"mean": float(e.mean()), "p99": float(np.percentile(e, 99)), "max": float(e.max())}
+            m = torch.from_numpy(synthetic.ellipsoid_mask(dims[i], (15, 12, 10))).to(dev)[None, None]
+            w_ours = warp(m, outs[i][None]) > 0.5
+            w_ref = warp(m, torch.from_numpy(ref[i].astype(np.float32)).to(dev)[None]) > 0.5
+            dices[key] = dice(w_ours[0, 0].float(), w_ref[0, 0].float())
+        vox = sum(int(np.prod(d)) for d in dims)
+        out.append({"storage": storage, "pairs_per_s": len(dims) / (ms / 1000.0), "ms_per_step": ms,
+                    "equivalent_80cube_pairs_per_s": vox / 512000.0 / (ms / 1000.0), "epe_vs_fp64_oracle": epe,
+                    "warped_mask_dice_vs_fp64_oracle": dices, "level_tiles": plan.level_tiles()[:3],
+                    "clocks": clocks})
+        plan.close()
+        solver._plans.clear()
+        torch.cuda.empty_cache()
+    print(json.dumps({"metric": "mixed-precision TV-L1 flow, 68 x 80^3 + 16 x 128^3 pairs",
+                      "unit": "pairs/s", "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
+                      "oracle": "FP64 C++ restatement on the host (oracle/svs_oracle.cpp), default configuration",
+                      "results": out}), flush=True)
+
+
+def run_serving(args):
+    """Poisson request streams (one request = a cine sequence with T uniform in 12..35 and dims per
+    axis uniform on {64, 72, ..., 128}) through the continuous-batching server (bf16-flow32 storage
+    unless --storage is given): p50/p99 latency from submit to flows and masks on the host, and
+    throughput, per arrival rate."""
+    import torch
+    from singleventriclesegmentation_b200 import synthetic
+    from singleventriclesegmentation_b200.serving import FlowServer
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    storage = args.storage if args.storage != "f16-flow32" else "bf16-flow32"
+    results = []
+    for rate in [float(r) for r in args.rates.split(",")]:
+        reqs = []
+        rng = np.random.default_rng(int(rate * 1000) + 1)
+        t = 0.0
+        for _ in range(args.requests):
+            t += rng.exponential(1.0 / rate)
+            T = int(rng.integers(12, 36))
+            dims = tuple(int(v) for v in rng.choice(np.arange(64, 129, 8), size=3))
+            reqs.append((t, T, dims))
+        data = []
+        for j, (_, T, dims) in enumerate(reqs):
+            frames = torch.from_numpy(synthetic.cine_sequence(T=T, shape=dims, seed=j, device="cuda")).pin_memory()
+            masks = torch.from_numpy(np.stack([synthetic.ellipsoid_mask(dims, (15, 12, 10)),
+                                               synthetic.ellipsoid_mask(dims, (13, 12, 10))])).pin_memory()
+            data.append((frames, masks, (0, min(12, T - 1))))
+        server = FlowServer(budget_bytes=100 << 30, storage=storage, device=dev)
+        t0 = time.perf_counter()
+        futs = []
+        for (ta, _, _), (frames, masks, mt) in zip(reqs, data):
+            delay = ta - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            futs.append(server.submit(frames, masks, mt))
+        for f in futs:
+            f.result()
+        server.close()
+        st = server.stats()
+        pairs = sum(2 * (T - 1) for _, T, _ in reqs)
+        span = st["completed"] / st["throughput_seq_per_s"] if st["throughput_seq_per_s"] else float("nan")
+        results.append({"rate_per_s": rate, "requests": len(reqs), "p50_s": st["p50_s"], "p99_s": st["p99_s"],
+                        "mean_s": st["mean_s"], "throughput_seq_per_s": st["throughput_seq_per_s"],
+                        "throughput_pairs_per_s": pairs / span, "max_concurrent": st["max_concurrent"],
+                        "sizes": [[T] + list(d) for _, T, d in reqs]})
+    print(json.dumps({"metric": "serving: per-sequence latency p50/p99 and throughput", "unit": "s",
+                      "storage": storage, "data": "synthetic", "budget_bytes": 100 << 30,
+                      "results": results}), flush=True)
+
+
 # ------------------------------------------------------------------------------ our arm
 def main():
     args = parse()
     if args.impl == "reference":
         reference_arm(args)
+        return
+    if args.workload != "sequence":
+        {"uneven": run_uneven, "mixed": run_mixed, "serving": run_serving}[args.workload](args)
         return
     import torch
     import torch.distributed as dist
@@ -231,6 +475,9 @@ def main():
     d_masks = host_masks.to(dev)
     flows = torch.empty((n_pairs,) + SHAPE + (3,), dtype=torch.float32, device=dev)
     plan = solver.plan_for([SHAPE] * n_pairs)
+    level_tiles_tuned = None
+    if not args.no_autotune:
+        level_tiles_tuned = tune_plan(plan, args.storage)
     fwd_idx = list(range(MASK_T0, MASK_T1))                       # forward pairs t -> t+1
     bwd_idx = [(T - 1) + (T - 1 - t) for t in range(MASK_T1, MASK_T0, -1)]  # backward pairs t -> t-1
 
@@ -293,21 +540,8 @@ def main():
     e2e_value = world * n_pairs * args.steps / (ms_e2e / 1000.0)
 
     # ----- the dominant kernel (fused iteration, level 0) timed alone on the live state
-    n_it = 30
-    plan.bench_iterations(0, 3)
-    torch.cuda.synchronize(dev)
-    e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e4.record(stream)
-    plan.bench_iterations(0, n_it)
-    e5.record(stream)
-    torch.cuda.synchronize(dev)
-    it_ms = e4.elapsed_time(e5) / n_it
-    # bytes per voxel-iteration: read u 3, p 9, D 6, rc 1, gw 3; write u 3, p 9
-    ub = 2 if args.storage in ("bf16", "f16") else 4
-    fb = 4 if args.storage == "f32" else 2
-    bpv = 6 * ub + 28 * fb
     vox0 = n_pairs * int(np.prod(SHAPE))
-    alg_bytes = vox0 * bpv
+    it_ms, alg_bytes = iterate_roofline(plan, args.storage, vox0, stream, dev)
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (it_ms / 1000.0) / 1e9
     traffic_pv = profiled_traffic().get(args.storage)
@@ -318,6 +552,11 @@ def main():
     bm = (chain[-1, 1, 0] > 0.5).float()
     mask_metrics = {"dice_fwd": dice(fm, d_masks[1, 0]), "hd_fwd": hausdorff(fm, d_masks[1, 0]),
                     "dice_bwd": dice(bm, d_masks[0, 0]), "hd_bwd": hausdorff(bm, d_masks[0, 0])}
+
+    plain = None
+    if rank == 0 and world == 1 and not args.no_plain_form:
+        plain = plain_form_rate(dev, d_seq)
+        plain["speedup_of_value"] = value / plain["value"]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -339,9 +578,10 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": None if traffic_pv is None else traffic_pv * vox0,
-                         "kernel": "iterate_kernel (fused primal-dual iteration), level 0",
+                         "kernel": "iterate kernel (fused primal-dual iteration, variant %d), level 0"
+                                   % plan.level_tiles()[0],
                          "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": it_ms},
-            "cpu_baseline": cpu, "clocks": clock_info, "masks": mask_metrics,
+            "cpu_baseline": cpu, "plain_gpu_form": plain, "clocks": clock_info, "masks": mask_metrics,
             "graph_kernels_per_solve": plan.graph_kernels,
         }
         print(json.dumps(line), flush=True)
