@@ -542,14 +542,29 @@ constexpr int split_id(int tx, int ty, int dist, int v) {
       return i + 1;
   return 0;
 }
-constexpr int kAutoF32 = split_id(32, 16, 3, 2), kAuto16 = split_id(16, 16, 3, 1);
-static_assert(kAutoF32 > 0 && kAuto16 > 0, "automatic variants are compiled");
+constexpr int kAutoF32 = split_id(32, 16, 3, 2), kAuto16 = split_id(16, 16, 3, 1),
+              kAuto16W40 = split_id(40, 8, 3, 2), kAuto16Narrow = split_id(32, 8, 3, 1);
+static_assert(kAutoF32 > 0 && kAuto16 > 0 && kAuto16W40 > 0 && kAuto16Narrow > 0,
+              "automatic variants are compiled");
 
-// Automatic choice (measured on B200 with 80^3 batches): split-role pipelines with prefetch
-// distance 3, 32x16 tiles of voxel pairs when the fields are 4-byte (one CTA per SM) and 16x16
-// tiles of single voxels when they are 2-byte (two CTAs per SM); the plain-load 32x8 form if TMA
-// descriptors cannot be built.
-int auto_tile(const svs_plan& P) { return P.prm.storage == SVS_STORAGE_F32 ? kAutoF32 : kAuto16; }
+// Automatic choice per level (measured on B200 with batches of 80^3 pairs, levels 80^3, 40^3 and
+// 20^3): split-role pipelines with prefetch distance 3. 4-byte fields: 32x16 tiles of voxel
+// pairs (one CTA per SM). 2-byte fields: 40x8 tiles of voxel pairs when every width is a
+// multiple of 40 (no idle lanes), 32x8 tiles of single voxels for widths up to 32, 16x16 tiles
+// of single voxels otherwise. The plain-load 32x8 form if TMA descriptors cannot be built. The
+// autotuner measures instead of assuming.
+int auto_tile(const svs_plan& P, int level) {
+  if (P.prm.storage == SVS_STORAGE_F32) return kAutoF32;
+  bool all40 = true;
+  int widest = 0;
+  for (int i = 0; i < P.num_pairs; ++i) {
+    const int nx = P.h_descs[(size_t)level * P.num_pairs + i].nx;
+    all40 = all40 && nx % 40 == 0;
+    widest = std::max(widest, nx);
+  }
+  if (all40) return kAuto16W40;
+  return widest <= 32 ? kAuto16Narrow : kAuto16;
+}
 
 void build_tiles(svs_plan& P, int level, int tid) {
   const TileShape ts = kTileShapes[tid - 1];
@@ -586,7 +601,7 @@ svs_status setup_tiles(svs_plan& P) {
   std::memset(maps.data(), 0, maps.size() * sizeof(TMaps));
   for (int l = 0; l < P.levels; ++l) {
     const int req = (l < (int)P.level_tile_req.size() && P.level_tile_req[l] > 0) ? P.level_tile_req[l] : want;
-    int tid = req > 0 ? req : auto_tile(P);
+    int tid = req > 0 ? req : auto_tile(P, l);
     build_tiles(P, l, tid);
     if (!iter_dispatch(P, &maps, l, tid, 0, nullptr, nullptr)) {
       if (req > 0) return fail(SVS_ERR_UNSUPPORTED, "tile variant not usable for this plan (shared memory or TMA descriptor limits)");
