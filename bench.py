@@ -62,6 +62,7 @@ def parse():
                          "oracle; serving: Poisson request stream through the continuous-batching server")
     ap.add_argument("--rates", default="0.1,1,10,50", help="serving: arrival rates (requests/s)")
     ap.add_argument("--requests", type=int, default=6, help="serving: requests per rate")
+    ap.add_argument("--max-active", type=int, default=2, help="serving: requests on the device at once")
     return ap.parse_args()
 
 
@@ -410,7 +411,7 @@ def run_serving(args):
             masks = torch.from_numpy(np.stack([synthetic.ellipsoid_mask(dims, (15, 12, 10)),
                                                synthetic.ellipsoid_mask(dims, (13, 12, 10))])).pin_memory()
             data.append((frames, masks, (0, min(12, T - 1))))
-        server = FlowServer(budget_bytes=100 << 30, storage=storage, device=dev)
+        server = FlowServer(budget_bytes=100 << 30, storage=storage, device=dev, max_active=args.max_active)
         t0 = time.perf_counter()
         futs = []
         for (ta, _, _), (frames, masks, mt) in zip(reqs, data):
@@ -423,13 +424,16 @@ def run_serving(args):
         server.close()
         st = server.stats()
         pairs = sum(2 * (T - 1) for _, T, _ in reqs)
+        eq80 = sum(2 * (T - 1) * int(np.prod(d)) for _, T, d in reqs) / 512000.0
         span = st["completed"] / st["throughput_seq_per_s"] if st["throughput_seq_per_s"] else float("nan")
         results.append({"rate_per_s": rate, "requests": len(reqs), "p50_s": st["p50_s"], "p99_s": st["p99_s"],
                         "mean_s": st["mean_s"], "throughput_seq_per_s": st["throughput_seq_per_s"],
-                        "throughput_pairs_per_s": pairs / span, "max_concurrent": st["max_concurrent"],
+                        "throughput_pairs_per_s": pairs / span,
+                        "throughput_80cube_equiv_pairs_per_s": eq80 / span, "max_concurrent": st["max_concurrent"],
                         "sizes": [[T] + list(d) for _, T, d in reqs]})
     print(json.dumps({"metric": "serving: per-sequence latency p50/p99 and throughput", "unit": "s",
                       "storage": storage, "data": "synthetic", "budget_bytes": 100 << 30,
+                      "max_active": args.max_active,
                       "results": results}), flush=True)
 
 

@@ -683,7 +683,7 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
   const long long col0 = (long long)gy * Dg.pitch + gx;
   SU* __restrict__ u_dst = reinterpret_cast<SU*>(Dg.u[a.src ^ 1]) + col0;
   SP* __restrict__ p_dst = reinterpret_cast<SP*>(Dg.p[a.src ^ 1]) + col0;
-  const int bdry = a.bdry;
+  const int bdry = GEN ? a.bdry : (int)SVS_BOUNDARY_MIRROR;  // GEN = false is launched for MIRROR only
   Stencil3 fx[V], ax[V];
 #pragma unroll
   for (int v = 0; v < V; ++v) {
@@ -806,9 +806,10 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
     const SU* Uk = ubox(k) + uo;
     const unsigned char* PD = smem + G::PD_OFF + ((k - kb) % G::NPD) * B::PD_SLOT;
     const Stencil3 fz = fwd_coef(k, nz, bdry, hz);
-    const bool has_m = k - 1 >= pl, has_p = k + 1 <= ph;
-    const SU* Um = ubox(has_m ? k - 1 : k) + uo;
-    const SU* Up = ubox(has_p ? k + 1 : k) + uo;
+    // planes k-1 and k+1 are missing only at k = 0 and k = nz-1, where the z stencil's
+    // coefficient for them is zero (every boundary type): plane k stands in for them
+    const SU* Um = ubox(k - 1 >= pl ? k - 1 : k) + uo;
+    const SU* Up = ubox(k + 1 <= ph ? k + 1 : k) + uo;
     if (role != 2) {
       if (active && !bad) {
         float dxy[V][3];
@@ -823,9 +824,9 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
           Lane<V, SU>::sh(Up + c * UC, n);
 #pragma unroll
           for (int v = 0; v < V; ++v) {
-            um[v][c] = has_m ? m[v] : 0.f;
+            um[v][c] = m[v];
             uc[v][c] = o[v];
-            up[v][c] = has_p ? n[v] : 0.f;
+            up[v][c] = n[v];
           }
         }
         const SP* P = reinterpret_cast<const SP*>(PD) + po;
@@ -917,8 +918,8 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
       for (int c = 0; c < 3; ++c) {
         const SU* u = Uk + c * UC;
         const float o = Store<SU>::sh(u);
-        const float m = has_m ? Store<SU>::sh(Um + c * UC) : 0.f;
-        const float n = has_p ? Store<SU>::sh(Up + c * UC) : 0.f;
+        const float m = Store<SU>::sh(Um + c * UC);
+        const float n = Store<SU>::sh(Up + c * UC);
         const float ex = apply3<GEN>(fx[0], Store<SU>::sh(u - 1), o, Store<SU>::sh(u + 1));
         const float ey = apply3<GEN>(fy, Store<SU>::sh(u - UXB), o, Store<SU>::sh(u + UXB));
         const float ez = apply3<GEN>(fz, m, o, n);
@@ -993,7 +994,8 @@ constexpr int kNumSplitShapes = sizeof(kSplitShapes) / sizeof(kSplitShapes[0]);
 
 // Split-role variant `idx` for a storage mode. op 0: set the kernels' shared-memory attribute
 // and return the TMA box shapes {u x, u y, p x, p y} in `box` (false if the variant does not
-// fit); op 1: launch one iteration over `ntiles` tiles on stream s.
+// fit); op 1: launch one iteration over `ntiles` tiles on stream s; op 2: resident CTAs per SM
+// in box[0] (after op 0).
 bool split_variant(int storage, int idx, int op, bool gen, unsigned ntiles, const Tile* tiles, const Desc* descs,
                    const TMaps* maps, const IterArgs* a, int* status, cudaStream_t s, int* box);
 

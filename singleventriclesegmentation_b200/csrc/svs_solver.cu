@@ -566,6 +566,36 @@ int auto_tile(const svs_plan& P, int level) {
   return widest <= 32 ? kAuto16Narrow : kAuto16;
 }
 
+// z chunks per column for a split-role variant: the count that minimises the launch's makespan
+// in plane steps, waves x (planes per chunk + kFillPlanes), where a wave is one CTA on every
+// resident slot (SMs x CTAs per SM from the occupancy calculator) and kFillPlanes stands for the
+// pipeline start of a chunk (the first DIST planes and the extra dual plane below z0).
+constexpr int kFillPlanes = 3;
+int split_chunks(const svs_plan& P, int level, int tid, long long xy_tiles) {
+  int dev = 0, sms = 148, per_sm = 0, nz = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int box[4] = {0, 0, 0, 0};
+  const TileShape& ts = kTileShapes[tid - 1];
+  if (!split_variant(P.prm.storage, ts.split, 2, P.prm.boundary != SVS_BOUNDARY_MIRROR, 0, nullptr, nullptr,
+                     nullptr, nullptr, nullptr, nullptr, box))
+    return 1;
+  per_sm = std::max(1, box[0]);
+  for (int i = 0; i < P.num_pairs; ++i) nz = std::max(nz, P.h_descs[(size_t)level * P.num_pairs + i].nz);
+  const long long slots = (long long)sms * per_sm;
+  int best = 1;
+  long long best_cost = -1;
+  for (int c = 1; c <= std::max(1, nz / 8); ++c) {
+    const long long waves = (xy_tiles * c + slots - 1) / slots;
+    const long long cost = waves * (ceil_div(nz, c) + kFillPlanes);
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      best = c;
+    }
+  }
+  return best;
+}
+
 void build_tiles(svs_plan& P, int level, int tid) {
   const TileShape ts = kTileShapes[tid - 1];
   std::vector<Tile>& out = P.h_tiles[level];
@@ -575,12 +605,16 @@ void build_tiles(svs_plan& P, int level, int tid) {
     const Desc& d = P.h_descs[(size_t)level * P.num_pairs + i];
     xy_tiles += (long long)ceil_div(d.nx, ts.tx) * ceil_div(d.ny, ts.ty);
   }
-  // z is split into chunks only when the level has too few column tiles to fill the GPU
+  // split-role variants: chunk count from the wave model above; other forms: z is split into
+  // chunks only when the level has too few column tiles to fill the GPU
+  const int split_c = ts.form == kSplit ? split_chunks(P, level, tid, xy_tiles) : 0;
   const long long target = 148LL * 2;
   for (int i = 0; i < P.num_pairs; ++i) {
     const Desc& d = P.h_descs[(size_t)level * P.num_pairs + i];
     int chunks = 1;
-    if (xy_tiles < target)
+    if (split_c > 0)
+      chunks = std::min(split_c, std::max(1, d.nz / 8));
+    else if (xy_tiles < target)
       chunks = (int)std::min<long long>((target + xy_tiles - 1) / xy_tiles, std::max(1, d.nz / 8));
     const int zc = (d.nz + chunks - 1) / chunks;
     for (int z0 = 0; z0 < d.nz; z0 += zc)
@@ -602,12 +636,12 @@ svs_status setup_tiles(svs_plan& P) {
   for (int l = 0; l < P.levels; ++l) {
     const int req = (l < (int)P.level_tile_req.size() && P.level_tile_req[l] > 0) ? P.level_tile_req[l] : want;
     int tid = req > 0 ? req : auto_tile(P, l);
-    build_tiles(P, l, tid);
+    // attributes and tensor maps first: the tile builder asks the occupancy calculator
     if (!iter_dispatch(P, &maps, l, tid, 0, nullptr, nullptr)) {
       if (req > 0) return fail(SVS_ERR_UNSUPPORTED, "tile variant not usable for this plan (shared memory or TMA descriptor limits)");
       tid = 6;  // plain-load 32x8
-      build_tiles(P, l, tid);
     }
+    build_tiles(P, l, tid);
     P.level_tile[l] = tid;
   }
   for (auto* p : P.d_tiles) cudaFree(p);

@@ -13,6 +13,16 @@ bool run(int op, bool gen, unsigned nt, const Tile* tiles, const Desc* descs, co
   using G = SplitGeom<SU, SP, S.tx, S.ty, S.dist, S.v>;
   auto* kf = iterate_split_kernel<SU, SP, S.tx, S.ty, S.dist, S.v, S.minb, false>;
   auto* kt = iterate_split_kernel<SU, SP, S.tx, S.ty, S.dist, S.v, S.minb, true>;
+  if (op == 2) {  // resident CTAs per SM (after op 0 set the shared-memory attribute)
+    if (G::SMEM > 227 * 1024) return false;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, gen ? kt : kf, G::NT, G::SMEM) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    box[0] = n;
+    return true;
+  }
   if (op == 0) {
     if (G::SMEM > 227 * 1024) return false;
     if (cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM) != cudaSuccess ||

@@ -1,7 +1,8 @@
 """A continuous-batching request loop for whole cine sequences.
 
 Each request is one sequence [T, Z, Y, X] (any size; optional end masks). The server admits
-requests while their device state fits a fixed HBM budget, gives each admitted request its own
+requests while their device state fits a fixed HBM budget (and at most max_active at once),
+gives each admitted request its own
 CUDA stream and a solver plan (pyramids, dual state and the captured graph stay on the device
 for the whole sequence), and starts the next waiting request as soon as an earlier one finishes
 and its memory is released, while the others keep running: the work of all admitted requests
@@ -61,9 +62,13 @@ class FlowServer:
     """Admission by HBM budget, one stream per admitted request, results on the host."""
 
     def __init__(self, budget_bytes: int = 40 << 30, storage: str = "f16-flow32", device=None,
-                 solver_args: Optional[dict] = None, poll_s: float = 0.002):
+                 solver_args: Optional[dict] = None, poll_s: float = 0.002, max_active: int = 2):
+        """max_active caps the requests on the device at once (memory permitting): one batched
+        sequence already fills the GPU, so more overlap adds latency to every request without
+        adding throughput; two keep the device busy across one request's host-side set-up."""
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.budget = int(budget_bytes)
+        self.max_active = max(1, int(max_active))
         self.storage = storage
         args = dict(num_scales=3, max_warps=15, max_outer_iterations=300, weight_matching=1.0, weight_tv=0.025,
                     primaldual_algorithm_type=2, primaldual_algorithm_params=(0.5, 0.5, 0.25, 1.0),
@@ -224,7 +229,7 @@ class FlowServer:
                         req.future.set_exception(e)
                     progressed = True
             with self._lock:
-                while self._waiting:
+                while self._waiting and len(self._active) < self.max_active:
                     req = self._waiting[0]
                     if self._in_use + req.bytes_needed > self.budget:
                         break

@@ -54,3 +54,17 @@ def test_budget_admits_as_memory_frees(cuda):
         big.submit(frames[0]).result(timeout=10)
     big.close()
 
+
+
+def test_active_request_cap(cuda):
+    frames = [seq(3, (16, 16, 24), s) for s in range(3)]
+    srv = FlowServer(budget_bytes=8 << 30, solver_args=SMALL, max_active=1)
+    futs = [srv.submit(f) for f in frames]
+    capped = [f.result(timeout=300) for f in futs]
+    srv.close()
+    assert srv.stats()["completed"] == 3 and srv.stats()["max_concurrent"] == 1
+    srv = FlowServer(budget_bytes=8 << 30, solver_args=SMALL, max_active=3)
+    free = [srv.submit(f).result(timeout=300) for f in frames]
+    srv.close()
+    for a, b in zip(capped, free):
+        assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])
