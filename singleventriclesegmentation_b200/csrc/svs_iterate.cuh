@@ -29,9 +29,33 @@
 
 namespace svs {
 
-struct Stencil3 {
-  float m, c, p;
+// Elementwise FP32 arithmetic on one voxel (float) or on two x-adjacent voxels at once (float2,
+// the packed FP32 instructions of sm_100). Every operation rounds like its scalar counterpart and
+// products are fused only where an explicit vfma says so, so the scalar and packed forms give
+// bitwise the same result per voxel.
+__device__ __forceinline__ float vfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ float vmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float vadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 vmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 vadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+template <typename T> __device__ __forceinline__ T bcast(float s);
+template <> __device__ __forceinline__ float bcast<float>(float s) { return s; }
+template <> __device__ __forceinline__ float2 bcast<float2>(float s) { return make_float2(s, s); }
+__device__ __forceinline__ float first(float v) { return v; }
+__device__ __forceinline__ float first(float2 v) { return v.x; }
+
+template <typename T>
+struct StencilV {
+  T m, c, p;
 };
+using Stencil3 = StencilV<float>;
+__device__ __forceinline__ StencilV<float2> pack(const Stencil3& a, const Stencil3& b) {
+  return {make_float2(a.m, b.m), make_float2(a.c, b.c), make_float2(a.p, b.p)};
+}
+template <typename T> __device__ __forceinline__ StencilV<T> bcast_st(const Stencil3& a) {
+  return {bcast<T>(a.m), bcast<T>(a.c), bcast<T>(a.p)};
+}
 
 __device__ __forceinline__ Stencil3 fwd_coef(int i, int n, int bdry, float h) {
   const float a = 0.5f / h;
@@ -53,45 +77,71 @@ __device__ __forceinline__ Stencil3 adj_coef(int i, int n, int bdry, float ih) {
 
 // GEN = false: MIRROR boundary, where every stencil has a zero centre coefficient (the centre
 // term is dropped; for h = 1 the result is bitwise that of the three-term form).
-template <bool GEN>
-__device__ __forceinline__ float apply3(const Stencil3& s, float prev, float cur, float next) {
-  if (GEN) return fmaf(s.p, next, fmaf(s.c, cur, s.m * prev));
-  return fmaf(s.p, next, s.m * prev);
+template <bool GEN, typename T>
+__device__ __forceinline__ T apply3(const StencilV<T>& s, T prev, T cur, T next) {
+  if (GEN) return vfma(s.p, next, vfma(s.c, cur, vmul(s.m, prev)));
+  return vfma(s.p, next, vmul(s.m, prev));
 }
 
-// Dual update of one flow component at one voxel, tvl13d.py:215-222 with
-// opticalFlowOps.cu:179-208: v = p + sigma D g; p_new = v / max(1, |v| / weight_tv), written as
-// v * min(1, weight_tv * rsqrt(|v|^2)).
-__device__ __forceinline__ void dual_row(const float D[6], float ex, float ey, float ez, float& p0,
-                                         float& p1, float& p2, float sigma, float wtv, float wtv2) {
-  const float d0 = D[0] * ex + D[1] * ey + D[2] * ez;
-  const float d1 = D[1] * ex + D[3] * ey + D[4] * ez;
-  const float d2 = D[2] * ex + D[4] * ey + D[5] * ez;
-  const float v0 = p0 + sigma * d0, v1 = p1 + sigma * d1, v2 = p2 + sigma * d2;
-  const float nsq = v0 * v0 + v1 * v1 + v2 * v2;
+// a0 b0 + a1 b1 + a2 b2
+template <typename T>
+__device__ __forceinline__ T dot3(T a0, T a1, T a2, T b0, T b1, T b2) {
+  return vfma(a2, b2, vfma(a1, b1, vmul(a0, b0)));
+}
+
+__device__ __forceinline__ float proj_scale(float nsq, float wtv, float wtv2) {
   // weight_tv == 0 gives sc = 0 (or v = 0), i.e. p = 0 as tvl13d.py:223-224 requires
-  const float sc = (nsq > wtv2) ? wtv * rsqrtf(nsq) : 1.0f;
-  p0 = v0 * sc;
-  p1 = v1 * sc;
-  p2 = v2 * sc;
+  return (nsq > wtv2) ? __fmul_rn(wtv, rsqrtf(nsq)) : 1.0f;
+}
+__device__ __forceinline__ float2 proj_scale(float2 nsq, float wtv, float wtv2) {
+  return make_float2(proj_scale(nsq.x, wtv, wtv2), proj_scale(nsq.y, wtv, wtv2));
 }
 
-// Primal update at one voxel, tvl13d.py:229-235 with opticalFlowOps.cu:123-175:
-// rho = rc + u.g (u before the update), u_new = (u - tau div) + shrinkage step.
-__device__ __forceinline__ void primal_voxel(const float u[3], const float div[3], float tau,
-                                             float factor, float rc, const float g[3], float un[3]) {
-  const float rho = rc + (u[0] * g[0] + u[1] * g[1] + u[2] * g[2]);
-  const float g2s = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) un[c] = u[c] - tau * div[c];
-  // the three cases of opticalFlowOps.cu:140-171 as one step length along g (no divergence):
-  // rho < -th: +factor; rho > th: -factor; |rho| <= th: -rho/|g|^2 (0 where |g|^2 <= 1e-10,
-  // the reference's (double)g2 > 1e-10 for a float g2)
-  const float th = factor * g2s;
-  const float t = (rho < -th) ? factor : (rho > th) ? -factor : (g2s >= 1e-10f ? __fdividef(-rho, g2s) : 0.f);
-#pragma unroll
-  for (int c = 0; c < 3; ++c) un[c] = fmaf(t, g[c], un[c]);
+// Dual update of one flow component, tvl13d.py:215-222 with opticalFlowOps.cu:179-208:
+// v = p + sigma D g; p_new = v / max(1, |v| / weight_tv), written as v * min(1, weight_tv *
+// rsqrt(|v|^2)). D is the packed symmetric tensor (d00 d01 d02 d11 d12 d22).
+template <typename T>
+__device__ __forceinline__ void dual_row(const T D[6], T ex, T ey, T ez, T& p0, T& p1, T& p2, float sigma,
+                                         float wtv, float wtv2) {
+  const T d0 = dot3(D[0], D[1], D[2], ex, ey, ez);
+  const T d1 = dot3(D[1], D[3], D[4], ex, ey, ez);
+  const T d2 = dot3(D[2], D[4], D[5], ex, ey, ez);
+  const T sg = bcast<T>(sigma);
+  const T v0 = vfma(sg, d0, p0), v1 = vfma(sg, d1, p1), v2 = vfma(sg, d2, p2);
+  const T sc = proj_scale(dot3(v0, v1, v2, v0, v1, v2), wtv, wtv2);
+  p0 = vmul(v0, sc);
+  p1 = vmul(v1, sc);
+  p2 = vmul(v2, sc);
 }
+
+// Step length along g of the L1 shrinkage, the three cases of opticalFlowOps.cu:140-171 (no
+// divergence): rho < -th: +factor; rho > th: -factor; |rho| <= th: -rho/|g|^2 (0 where
+// |g|^2 <= 1e-10, the reference's (double)g2 > 1e-10 for a float g2).
+__device__ __forceinline__ float shrink_step(float rho, float g2s, float factor) {
+  const float th = __fmul_rn(factor, g2s);
+  return (rho < -th) ? factor : (rho > th) ? -factor : (g2s >= 1e-10f ? __fdividef(-rho, g2s) : 0.f);
+}
+__device__ __forceinline__ float2 shrink_step(float2 rho, float2 g2s, float factor) {
+  return make_float2(shrink_step(rho.x, g2s.x, factor), shrink_step(rho.y, g2s.y, factor));
+}
+
+// Primal update, tvl13d.py:229-235 with opticalFlowOps.cu:123-175: rho = rc + u.g (u before
+// the update), u_new = (u - tau div) + shrinkage step along g.
+template <typename T>
+__device__ __forceinline__ void primal_voxel(const T u[3], const T div[3], float tau, float factor, T rc,
+                                             const T g[3], T un[3]) {
+  const T rho = vadd(rc, dot3(u[0], u[1], u[2], g[0], g[1], g[2]));
+  const T g2s = dot3(g[0], g[1], g[2], g[0], g[1], g[2]);
+  const T mt = bcast<T>(-tau);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) un[c] = vfma(mt, div[c], u[c]);
+  const T t = shrink_step(rho, g2s, factor);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) un[c] = vfma(t, g[c], un[c]);
+}
+
+// div = (dx + dy) + dz
+template <typename T> __device__ __forceinline__ T sum3(T dx, T dy, T dz) { return vadd(vadd(dx, dy), dz); }
 
 // ------------------------------------------------------------------------ plain-load form
 template <typename SU, typename SP, int TX, int TY, bool GEN>
@@ -203,9 +253,9 @@ iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, I
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        sq[slot][c][ty][tx] = Dk[0] * pk[3 * c] + Dk[1] * pk[3 * c + 1] + Dk[2] * pk[3 * c + 2];
-        sq[slot][3 + c][ty][tx] = Dk[1] * pk[3 * c] + Dk[3] * pk[3 * c + 1] + Dk[4] * pk[3 * c + 2];
-        qzc[c] = Dk[2] * pk[3 * c] + Dk[4] * pk[3 * c + 1] + Dk[5] * pk[3 * c + 2];
+        sq[slot][c][ty][tx] = dot3(Dk[0], Dk[1], Dk[2], pk[3 * c], pk[3 * c + 1], pk[3 * c + 2]);
+        sq[slot][3 + c][ty][tx] = dot3(Dk[1], Dk[3], Dk[4], pk[3 * c], pk[3 * c + 1], pk[3 * c + 2]);
+        qzc[c] = dot3(Dk[2], Dk[4], Dk[5], pk[3 * c], pk[3 * c + 1], pk[3 * c + 2]);
       }
     }
     if (primal_on) {
@@ -216,7 +266,7 @@ iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, I
       for (int c = 0; c < 3; ++c) {
         const float dx = apply3<GEN>(ax, sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1]);
         const float dy = apply3<GEN>(ay, sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx]);
-        div[c] = (dx + dy) + apply3<GEN>(az, qzmm[c], qzm[c], qzc[c]);
+        div[c] = sum3(dx, dy, apply3<GEN>(az, qzmm[c], qzm[c], qzc[c]));
       }
       primal_voxel(um, div, a.tau, a.factor, rcj, gj, un);
       const int o = j * plane + col;
@@ -251,7 +301,7 @@ iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, I
       for (int c = 0; c < 3; ++c) {
         const float dx = apply3<GEN>(ax, sq[ps][c][ty][tx - 1], sq[ps][c][ty][tx], sq[ps][c][ty][tx + 1]);
         const float dy = apply3<GEN>(ay, sq[ps][3 + c][ty - 1][tx], sq[ps][3 + c][ty][tx], sq[ps][3 + c][ty + 1][tx]);
-        div[c] = (dx + dy) + apply3<GEN>(az, qzmm[c], qzm[c], 0.f);
+        div[c] = sum3(dx, dy, apply3<GEN>(az, qzmm[c], qzm[c], 0.f));
       }
       primal_voxel(um, div, a.tau, a.factor, rcj, gj, un);
 #pragma unroll
@@ -484,9 +534,9 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        sq[qs][c][ty][tx] = Dk[0] * pk[3 * c] + Dk[1] * pk[3 * c + 1] + Dk[2] * pk[3 * c + 2];
-        sq[qs][3 + c][ty][tx] = Dk[1] * pk[3 * c] + Dk[3] * pk[3 * c + 1] + Dk[4] * pk[3 * c + 2];
-        qzc[c] = Dk[2] * pk[3 * c] + Dk[4] * pk[3 * c + 1] + Dk[5] * pk[3 * c + 2];
+        sq[qs][c][ty][tx] = dot3(Dk[0], Dk[1], Dk[2], pk[3 * c], pk[3 * c + 1], pk[3 * c + 2]);
+        sq[qs][3 + c][ty][tx] = dot3(Dk[1], Dk[3], Dk[4], pk[3 * c], pk[3 * c + 1], pk[3 * c + 2]);
+        qzc[c] = dot3(Dk[2], Dk[4], Dk[5], pk[3 * c], pk[3 * c + 1], pk[3 * c + 2]);
       }
     }
     // every thread is done with planes < k-1 (u, rc/gw) and with the p/D of plane k
@@ -512,7 +562,7 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
         gj[c] = Store<SP>::sh(GW + c * TY * TX);
         const float dx = apply3<GEN>(ax, sq[ps][c][ty][tx - 1], GEN ? sq[ps][c][ty][tx] : 0.f, sq[ps][c][ty][tx + 1]);
         const float dy = apply3<GEN>(ay, sq[ps][3 + c][ty - 1][tx], GEN ? sq[ps][3 + c][ty][tx] : 0.f, sq[ps][3 + c][ty + 1][tx]);
-        div[c] = (dx + dy) + apply3<GEN>(az, qzmm[c], qzm[c], qzc[c]);
+        div[c] = sum3(dx, dy, apply3<GEN>(az, qzmm[c], qzm[c], qzc[c]));
       }
       primal_voxel(uown_m, div, a.tau, a.factor, rcj, gj, un);
       SU* dst = u_dst + j * plane;
@@ -553,7 +603,7 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
         gj[c] = Store<SP>::sh(GW + c * TY * TX);
         const float dx = apply3<GEN>(ax, sq[ps][c][ty][tx - 1], GEN ? sq[ps][c][ty][tx] : 0.f, sq[ps][c][ty][tx + 1]);
         const float dy = apply3<GEN>(ay, sq[ps][3 + c][ty - 1][tx], GEN ? sq[ps][3 + c][ty][tx] : 0.f, sq[ps][3 + c][ty + 1][tx]);
-        div[c] = (dx + dy) + apply3<GEN>(az, qzmm[c], qzm[c], 0.f);
+        div[c] = sum3(dx, dy, apply3<GEN>(az, qzmm[c], qzm[c], 0.f));
       }
       primal_voxel(uown_m, div, a.tau, a.factor, rcj, gj, un);
       SU* dst = u_dst + j * plane;
@@ -581,33 +631,32 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
 // The arithmetic of every voxel is the expression sequence of iterate_tma_kernel, so the two
 // kernels give bitwise the same result. q rows live in qx [TY][TX+4] (x from x0-2, so V-voxel
 // groups start on even indices) and qy [TY+2][TX] (rows from y0-1).
+// Value type of a lane: one voxel (float) or two x-adjacent voxels (float2, packed FP32 math).
+template <int V> using LaneT = typename std::conditional<V == 2, float2, float>::type;
+// Load / store the lane's V voxels of storage type S (for V = 2: one 8-byte f32 or 4-byte 16-bit
+// access; the roundings are those of Store<S> per value).
 template <int V, typename S> struct Lane;
 template <typename S> struct Lane<1, S> {
-  static __device__ __forceinline__ void sh(const S* p, float (&o)[1]) { o[0] = Store<S>::sh(p); }
-  static __device__ __forceinline__ void st(S* p, const float (&v)[1]) { Store<S>::st(p, v[0]); }
+  static __device__ __forceinline__ float ld(const S* p) { return Store<S>::sh(p); }
+  static __device__ __forceinline__ void st(S* p, float v) { Store<S>::st(p, v); }
 };
 template <typename S> struct Lane<2, S> {
-  static __device__ __forceinline__ void sh(const S* p, float (&o)[2]) {
-    const float2 t = Pair<S>::sh(p);
-    o[0] = t.x;
-    o[1] = t.y;
-  }
-  static __device__ __forceinline__ void st(S* p, const float (&v)[2]) { Pair<S>::st(p, v[0], v[1]); }
+  static __device__ __forceinline__ float2 ld(const S* p) { return Pair<S>::sh(p); }
+  static __device__ __forceinline__ void st(S* p, float2 v) { Pair<S>::st(p, v.x, v.y); }
 };
 template <> struct Lane<1, float> {
-  static __device__ __forceinline__ void sh(const float* p, float (&o)[1]) { o[0] = *p; }
-  static __device__ __forceinline__ void st(float* p, const float (&v)[1]) { *p = v[0]; }
+  static __device__ __forceinline__ float ld(const float* p) { return *p; }
+  static __device__ __forceinline__ void st(float* p, float v) { *p = v; }
 };
 template <> struct Lane<2, float> {
-  static __device__ __forceinline__ void sh(const float* p, float (&o)[2]) {
-    const float2 t = *reinterpret_cast<const float2*>(p);
-    o[0] = t.x;
-    o[1] = t.y;
-  }
-  static __device__ __forceinline__ void st(float* p, const float (&v)[2]) {
-    *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
-  }
+  static __device__ __forceinline__ float2 ld(const float* p) { return *reinterpret_cast<const float2*>(p); }
+  static __device__ __forceinline__ void st(float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
 };
+// x-neighbours of the lane's voxels: L is the value left of the first voxel, R right of the last
+__device__ __forceinline__ float prev_x(float L, float) { return L; }
+__device__ __forceinline__ float next_x(float, float R) { return R; }
+__device__ __forceinline__ float2 prev_x(float L, float2 o) { return make_float2(L, o.x); }
+__device__ __forceinline__ float2 next_x(float2 o, float R) { return make_float2(o.y, R); }
 
 template <typename SU, typename SP, int TX, int TY, int DIST, int V>
 struct SplitGeom {
@@ -639,6 +688,7 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
                      const TMaps* __restrict__ maps, IterArgs a, int* __restrict__ status) {
   using G = SplitGeom<SU, SP, TX, TY, DIST, V>;
   using B = typename G::B;
+  using T = LaneT<V>;
   constexpr int AU = B::AU, AP = B::AP, UXB = B::UXB, PXB = B::PXB;
   constexpr int UC = B::UYB * UXB, PC = B::PYB * PXB, RCS = TY * TX, SXW = G::SXW;
   static_assert(DIST >= 2, "step k waits for plane k+1, issued at the end of step k+1-DIST");
@@ -647,13 +697,13 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
   float(*sqy)[3][TY + 2][TX] = reinterpret_cast<float(*)[3][TY + 2][TX]>(smem + G::SQY_OFF);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + G::BAR_OFF);
 
-  const Tile T = tiles[blockIdx.x];
-  const Desc& Dg = descs[T.desc];
-  const TMaps* M = maps + T.desc;
+  const Tile Tl = tiles[blockIdx.x];
+  const Desc& Dg = descs[Tl.desc];
+  const TMaps* M = maps + Tl.desc;
   const int nz = Dg.nz, ny = Dg.ny, nx = Dg.nx;
   const int cs = (int)Dg.cs;
   const int plane = Dg.pitch * ny;
-  const int z0 = T.z0z1 & 0xffff, z1 = T.z0z1 >> 16;
+  const int z0 = Tl.z0z1 & 0xffff, z1 = Tl.z0z1 >> 16;
   const CUtensorMap* mu = &M->u[a.src];
   const CUtensorMap* mp = &M->p[a.src];
 
@@ -674,7 +724,7 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
     lx = (h < TY) ? -1 : TX;
     ly = h % TY;
   }
-  const int gx = T.x0 + lx, gy = T.y0 + ly;
+  const int gx = Tl.x0 + lx, gy = Tl.y0 + ly;
   const bool active = gx >= 0 && gx < nx && gy >= 0 && gy < ny;
   const bool full = gx + V - 1 < nx;          // roles 0/1: every voxel of the lane is inside
   const int uo = (ly + 2) * UXB + (lx + AU);  // own (first) voxel in a u box component
@@ -684,14 +734,17 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
   SU* __restrict__ u_dst = reinterpret_cast<SU*>(Dg.u[a.src ^ 1]) + col0;
   SP* __restrict__ p_dst = reinterpret_cast<SP*>(Dg.p[a.src ^ 1]) + col0;
   const int bdry = GEN ? a.bdry : (int)SVS_BOUNDARY_MIRROR;  // GEN = false is launched for MIRROR only
-  Stencil3 fx[V], ax[V];
-#pragma unroll
-  for (int v = 0; v < V; ++v) {
-    fx[v] = fwd_coef(gx + v, nx, bdry, Dg.hx);
-    ax[v] = adj_coef(gx + v, nx, bdry, 1.0f / Dg.hx);
+  const Stencil3 fx0 = fwd_coef(gx, nx, bdry, Dg.hx), ax0 = adj_coef(gx, nx, bdry, 1.0f / Dg.hx);
+  StencilV<T> fx, ax;
+  if constexpr (V == 2) {
+    fx = pack(fx0, fwd_coef(gx + 1, nx, bdry, Dg.hx));
+    ax = pack(ax0, adj_coef(gx + 1, nx, bdry, 1.0f / Dg.hx));
+  } else {
+    fx = fx0;
+    ax = ax0;
   }
-  const Stencil3 fy = fwd_coef(gy, ny, bdry, Dg.hy);
-  const Stencil3 ay = adj_coef(gy, ny, bdry, 1.0f / Dg.hy);
+  const Stencil3 fy1 = fwd_coef(gy, ny, bdry, Dg.hy);
+  const StencilV<T> fy = bcast_st<T>(fy1), ay = bcast_st<T>(adj_coef(gy, ny, bdry, 1.0f / Dg.hy));
   const float ihz = 1.0f / Dg.hz, hz = Dg.hz;
 
   const int kb = max(z0 - 1, 0), ke = min(z1, nz - 1);
@@ -702,17 +755,17 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
     unsigned char* U = smem + G::U_OFF + (r % G::NU) * B::U_SLOT;
     if (q < kb) {
       mbar_arrive_expect_tx(bar, (uint32_t)B::U_TX);
-      tma_load_4d(U, mu, bar, T.x0 - AU, T.y0 - 2, q, 0);
+      tma_load_4d(U, mu, bar, Tl.x0 - AU, Tl.y0 - 2, q, 0);
       return;
     }
     unsigned char* PD = smem + G::PD_OFF + ((q - kb) % G::NPD) * B::PD_SLOT;
     unsigned char* R = smem + G::R_OFF + ((q - kb) % G::NR) * B::R_SLOT;
     mbar_arrive_expect_tx(bar, (uint32_t)B::FULL_TX);
-    tma_load_4d(U, mu, bar, T.x0 - AU, T.y0 - 2, q, 0);
-    tma_load_4d(PD, mp, bar, T.x0 - AP, T.y0 - 1, q, 0);
-    tma_load_4d(PD + B::P_SLOT, &M->D, bar, T.x0 - AP, T.y0 - 1, q, 0);
-    tma_load_4d(R, &M->rc, bar, T.x0, T.y0, q, 0);
-    tma_load_4d(R + B::RC_SLOT, &M->gw, bar, T.x0, T.y0, q, 0);
+    tma_load_4d(U, mu, bar, Tl.x0 - AU, Tl.y0 - 2, q, 0);
+    tma_load_4d(PD, mp, bar, Tl.x0 - AP, Tl.y0 - 1, q, 0);
+    tma_load_4d(PD + B::P_SLOT, &M->D, bar, Tl.x0 - AP, Tl.y0 - 1, q, 0);
+    tma_load_4d(R, &M->rc, bar, Tl.x0, Tl.y0, q, 0);
+    tma_load_4d(R + B::RC_SLOT, &M->gw, bar, Tl.x0, Tl.y0, q, 0);
   };
   auto ubox = [&](int q) {
     return reinterpret_cast<const SU*>(smem + G::U_OFF + ((q - pl) % G::NU) * B::U_SLOT);
@@ -738,58 +791,46 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
   bool bad = false;
 
   // q_z of the own voxels (role 0) at planes k-2, k-1, k
-  float qmm[V][3] = {}, qm[V][3] = {}, qc[V][3] = {};
+  T qmm[3], qm[3], qc[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) qmm[c] = qm[c] = qc[c] = bcast<T>(0.f);
   const float wtv2 = a.wtv * a.wtv;
 
   // x/y part of the divergence at plane j (q rows of slot j & 1), loaded before the dual
-  auto load_dxy = [&](int j, float (&dxy)[V][3]) {
+  auto load_dxy = [&](int j, T (&dxy)[3]) {
     const int ps = j & 1;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const float* qx = &sqx[ps][c][ly][lx + 2];
-      float o[V], dn[V], up[V], oy[V];
-      Lane<V, float>::sh(qx, o);
-      const float L = qx[-1], R = qx[V];
-      Lane<V, float>::sh(&sqy[ps][c][ly][lx], dn);
-      Lane<V, float>::sh(&sqy[ps][c][ly + 2][lx], up);
-      if (GEN) Lane<V, float>::sh(&sqy[ps][c][ly + 1][lx], oy);
-#pragma unroll
-      for (int v = 0; v < V; ++v) {
-        const float prev = v == 0 ? L : o[v - 1], next = v == V - 1 ? R : o[v + 1];
-        const float dx = apply3<GEN>(ax[v], prev, GEN ? o[v] : 0.f, next);
-        dxy[v][c] = dx + apply3<GEN>(ay, dn[v], GEN ? oy[v] : 0.f, up[v]);
-      }
+      const T o = Lane<V, float>::ld(qx);
+      const T dx = apply3<GEN>(ax, prev_x(qx[-1], o), GEN ? o : bcast<T>(0.f), next_x(o, qx[V]));
+      const T dn = Lane<V, float>::ld(&sqy[ps][c][ly][lx]);
+      const T up = Lane<V, float>::ld(&sqy[ps][c][ly + 2][lx]);
+      const T oy = GEN ? Lane<V, float>::ld(&sqy[ps][c][ly + 1][lx]) : bcast<T>(0.f);
+      dxy[c] = vadd(dx, apply3<GEN>(ay, dn, oy, up));
     }
   };
   // primal of plane j: qn = q_z(j+1), uj = own u at plane j
-  auto finish_primal = [&](int j, const float (&dxy)[V][3], const float (&qn)[V][3], const float (&uj)[V][3]) {
+  auto finish_primal = [&](int j, const T (&dxy)[3], const T (&qn)[3], const T (&uj)[3]) {
     const unsigned char* R = rbox(j);
     const SP* RC = reinterpret_cast<const SP*>(R) + ro;
     const SP* GW = reinterpret_cast<const SP*>(R + B::RC_SLOT) + ro;
-    const Stencil3 az = adj_coef(j, nz, bdry, ihz);
-    float rc[V], g[3][V], n[3][V];
-    Lane<V, SP>::sh(RC, rc);
+    const StencilV<T> az = bcast_st<T>(adj_coef(j, nz, bdry, ihz));
+    const T rc = Lane<V, SP>::ld(RC);
+    T g[3], d[3], n[3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) Lane<V, SP>::sh(GW + c * RCS, g[c]);
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      float d[3], gv[3], nv[3];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        d[c] = dxy[v][c] + apply3<GEN>(az, qmm[v][c], qm[v][c], qn[v][c]);
-        gv[c] = g[c][v];
-      }
-      primal_voxel(uj[v], d, a.tau, a.factor, rc[v], gv, nv);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) n[c][v] = nv[c];
+    for (int c = 0; c < 3; ++c) {
+      g[c] = Lane<V, SP>::ld(GW + c * RCS);
+      d[c] = vadd(dxy[c], apply3<GEN>(az, qmm[c], qm[c], qn[c]));
     }
+    primal_voxel(uj, d, a.tau, a.factor, rc, g, n);
     SU* dst = u_dst + (long long)j * plane;
     if (full) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) Lane<V, SU>::st(dst + c * cs, n[c]);
     } else {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) Store<SU>::st(dst + c * cs, n[c][0]);
+      for (int c = 0; c < 3; ++c) Store<SU>::st(dst + c * cs, first(n[c]));
     }
   };
 
@@ -805,108 +846,62 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
     const int qs = k & 1;
     const SU* Uk = ubox(k) + uo;
     const unsigned char* PD = smem + G::PD_OFF + ((k - kb) % G::NPD) * B::PD_SLOT;
-    const Stencil3 fz = fwd_coef(k, nz, bdry, hz);
+    const Stencil3 fz1 = fwd_coef(k, nz, bdry, hz);
     // planes k-1 and k+1 are missing only at k = 0 and k = nz-1, where the z stencil's
     // coefficient for them is zero (every boundary type): plane k stands in for them
     const SU* Um = ubox(k - 1 >= pl ? k - 1 : k) + uo;
     const SU* Up = ubox(k + 1 <= ph ? k + 1 : k) + uo;
     if (role != 2) {
       if (active && !bad) {
-        float dxy[V][3];
+        const StencilV<T> fz = bcast_st<T>(fz1);
+        T dxy[3];
         if (WP && role == 0) load_dxy(k - 1, dxy);
-        // own voxels at planes k-1, k, k+1
-        float um[V][3], uc[V][3], up[V][3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          float m[V], o[V], n[V];
-          Lane<V, SU>::sh(Um + c * UC, m);
-          Lane<V, SU>::sh(Uk + c * UC, o);
-          Lane<V, SU>::sh(Up + c * UC, n);
-#pragma unroll
-          for (int v = 0; v < V; ++v) {
-            um[v][c] = m[v];
-            uc[v][c] = o[v];
-            up[v][c] = n[v];
-          }
-        }
         const SP* P = reinterpret_cast<const SP*>(PD) + po;
         const SP* Dm = reinterpret_cast<const SP*>(PD + B::P_SLOT) + po;
-        float pv[9][V], Dv[6][V];
+        T pk[9], Dk[6], um[3];
 #pragma unroll
-        for (int c = 0; c < 9; ++c) Lane<V, SP>::sh(P + c * PC, pv[c]);
+        for (int c = 0; c < 9; ++c) pk[c] = Lane<V, SP>::ld(P + c * PC);
 #pragma unroll
-        for (int c = 0; c < 6; ++c) Lane<V, SP>::sh(Dm + c * PC, Dv[c]);
-        float pk[V][9], Dk[V][6];
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-#pragma unroll
-          for (int c = 0; c < 9; ++c) pk[v][c] = pv[c][v];
-#pragma unroll
-          for (int c = 0; c < 6; ++c) Dk[v][c] = Dv[c][v];
-        }
+        for (int c = 0; c < 6; ++c) Dk[c] = Lane<V, SP>::ld(Dm + c * PC);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const SU* u = Uk + c * UC;
-          const float L = Store<SU>::sh(u - 1), R = Store<SU>::sh(u + V);
-          float dn[V], upy[V];
-          Lane<V, SU>::sh(u - UXB, dn);
-          Lane<V, SU>::sh(u + UXB, upy);
-#pragma unroll
-          for (int v = 0; v < V; ++v) {
-            const float prev = v == 0 ? L : uc[v - 1][c], next = v == V - 1 ? R : uc[v + 1][c];
-            const float ex = apply3<GEN>(fx[v], prev, uc[v][c], next);
-            const float ey = apply3<GEN>(fy, dn[v], uc[v][c], upy[v]);
-            const float ez = apply3<GEN>(fz, um[v][c], uc[v][c], up[v][c]);
-            dual_row(Dk[v], ex, ey, ez, pk[v][3 * c], pk[v][3 * c + 1], pk[v][3 * c + 2], a.sigma, a.wtv, wtv2);
-          }
+          const T o = Lane<V, SU>::ld(u);
+          um[c] = Lane<V, SU>::ld(Um + c * UC);
+          const T ex = apply3<GEN>(fx, prev_x(Store<SU>::sh(u - 1), o), o, next_x(o, Store<SU>::sh(u + V)));
+          const T ey = apply3<GEN>(fy, Lane<V, SU>::ld(u - UXB), o, Lane<V, SU>::ld(u + UXB));
+          const T ez = apply3<GEN>(fz, um[c], o, Lane<V, SU>::ld(Up + c * UC));
+          dual_row(Dk, ex, ey, ez, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2], a.sigma, a.wtv, wtv2);
         }
         if (role == 0) {
           if (k >= z0 && k < z1) {
             SP* dst = p_dst + (long long)k * plane;
             if (full) {
 #pragma unroll
-              for (int c = 0; c < 9; ++c) {
-                float t[V];
-#pragma unroll
-                for (int v = 0; v < V; ++v) t[v] = pk[v][c];
-                Lane<V, SP>::st(dst + c * cs, t);
-              }
+              for (int c = 0; c < 9; ++c) Lane<V, SP>::st(dst + c * cs, pk[c]);
             } else {
 #pragma unroll
-              for (int c = 0; c < 9; ++c) Store<SP>::st(dst + c * cs, pk[0][c]);
+              for (int c = 0; c < 9; ++c) Store<SP>::st(dst + c * cs, first(pk[c]));
             }
           }
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
-            float qx[V], qy[V];
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-              const float* D = Dk[v];
-              const float* p = &pk[v][3 * c];
-              qx[v] = D[0] * p[0] + D[1] * p[1] + D[2] * p[2];
-              qy[v] = D[1] * p[0] + D[3] * p[1] + D[4] * p[2];
-              qc[v][c] = D[2] * p[0] + D[4] * p[1] + D[5] * p[2];
-            }
-            Lane<V, float>::st(&sqx[qs][c][ly][lx + 2], qx);
-            Lane<V, float>::st(&sqy[qs][c][ly + 1][lx], qy);
+            const T* pc = &pk[3 * c];
+            Lane<V, float>::st(&sqx[qs][c][ly][lx + 2], dot3(Dk[0], Dk[1], Dk[2], pc[0], pc[1], pc[2]));
+            Lane<V, float>::st(&sqy[qs][c][ly + 1][lx], dot3(Dk[1], Dk[3], Dk[4], pc[0], pc[1], pc[2]));
+            qc[c] = dot3(Dk[2], Dk[4], Dk[5], pc[0], pc[1], pc[2]);
           }
           if (WP) finish_primal(k - 1, dxy, qc, um);
         } else {
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
-            float qy[V];
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-              const float* D = Dk[v];
-              const float* p = &pk[v][3 * c];
-              qy[v] = D[1] * p[0] + D[3] * p[1] + D[4] * p[2];
-            }
-            Lane<V, float>::st(&sqy[qs][c][ly + 1][lx], qy);
+            const T* pc = &pk[3 * c];
+            Lane<V, float>::st(&sqy[qs][c][ly + 1][lx], dot3(Dk[1], Dk[3], Dk[4], pc[0], pc[1], pc[2]));
           }
         }
       }
     } else if (active && !bad) {
-      // halo column: one voxel
+      // halo column: one voxel, scalar arithmetic
       const SP* P = reinterpret_cast<const SP*>(PD) + po;
       const SP* Dm = reinterpret_cast<const SP*>(PD + B::P_SLOT) + po;
       float pk[9], Dk[6];
@@ -918,16 +913,14 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
       for (int c = 0; c < 3; ++c) {
         const SU* u = Uk + c * UC;
         const float o = Store<SU>::sh(u);
-        const float m = Store<SU>::sh(Um + c * UC);
-        const float n = Store<SU>::sh(Up + c * UC);
-        const float ex = apply3<GEN>(fx[0], Store<SU>::sh(u - 1), o, Store<SU>::sh(u + 1));
-        const float ey = apply3<GEN>(fy, Store<SU>::sh(u - UXB), o, Store<SU>::sh(u + UXB));
-        const float ez = apply3<GEN>(fz, m, o, n);
+        const float ex = apply3<GEN>(fx0, Store<SU>::sh(u - 1), o, Store<SU>::sh(u + 1));
+        const float ey = apply3<GEN>(fy1, Store<SU>::sh(u - UXB), o, Store<SU>::sh(u + UXB));
+        const float ez = apply3<GEN>(fz1, Store<SU>::sh(Um + c * UC), o, Store<SU>::sh(Up + c * UC));
         dual_row(Dk, ex, ey, ez, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2], a.sigma, a.wtv, wtv2);
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c)
-        sqx[qs][c][ly][lx + 2] = Dk[0] * pk[3 * c] + Dk[1] * pk[3 * c + 1] + Dk[2] * pk[3 * c + 2];
+        sqx[qs][c][ly][lx + 2] = dot3(Dk[0], Dk[1], Dk[2], pk[3 * c], pk[3 * c + 1], pk[3 * c + 2]);
     }
     // everyone is done with plane k's p/D, plane k-1's u and rc/gw, and q rows of plane k-1
     if (__syncthreads_or(bad)) {
@@ -939,12 +932,10 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
       issued = k + DIST;
     }
 #pragma unroll
-    for (int v = 0; v < V; ++v)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        qmm[v][c] = qm[v][c];
-        qm[v][c] = qc[v][c];
-      }
+    for (int c = 0; c < 3; ++c) {
+      qmm[c] = qm[c];
+      qm[c] = qc[c];
+    }
   };
 
   // the first one or two steps have no finished plane (j = k-1 < z0)
@@ -966,15 +957,10 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
   if (z1 >= nz) {
     const int j = nz - 1;
     if (role == 0 && active && j >= z0) {
-      float dxy[V][3], uj[V][3];
-      const float zero[V][3] = {};
+      T dxy[3], uj[3];
+      const T zero[3] = {bcast<T>(0.f), bcast<T>(0.f), bcast<T>(0.f)};
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        float o[V];
-        Lane<V, SU>::sh(ubox(j) + uo + c * UC, o);
-#pragma unroll
-        for (int v = 0; v < V; ++v) uj[v][c] = o[v];
-      }
+      for (int c = 0; c < 3; ++c) uj[c] = Lane<V, SU>::ld(ubox(j) + uo + c * UC);
       load_dxy(j, dxy);
       finish_primal(j, dxy, zero, uj);
     }
