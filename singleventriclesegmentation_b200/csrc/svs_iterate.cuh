@@ -349,6 +349,24 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     if (global_ns() - t0 > kMbarWaitNs) return false;
   return true;
 }
+// Plain arrival (release, CTA scope) of this thread on an mbarrier.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+// Bounded wait that also gives up as soon as another thread of the CTA has raised `abort`; a
+// thread that times out raises it.
+__device__ __forceinline__ bool mbar_wait_abort(uint64_t* bar, uint32_t parity, volatile int* abort) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (*abort) return false;
+    if (global_ns() - t0 > kMbarWaitNs) {
+      *abort = 1;
+      return false;
+    }
+  }
+  return true;
+}
 // 4D tiled TMA load (no multicast) of one box into shared memory, completion on `bar`.
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, uint64_t* bar, int x,
                                             int y, int z, int c) {
@@ -658,7 +676,7 @@ __device__ __forceinline__ float next_x(float, float R) { return R; }
 __device__ __forceinline__ float2 prev_x(float L, float2 o) { return make_float2(L, o.x); }
 __device__ __forceinline__ float2 next_x(float2 o, float R) { return make_float2(o.y, R); }
 
-template <typename SU, typename SP, int TX, int TY, int DIST, int V>
+template <typename SU, typename SP, int TX, int TY, int DIST, int V, bool AS = false>
 struct SplitGeom {
   using B = TmaGeom<SU, SP, TX, TY, DIST>;  // box shapes (shared with the tensor maps)
   static_assert(V == 1 || V == 2, "one or two voxels per lane");
@@ -679,14 +697,19 @@ struct SplitGeom {
   static constexpr int SQY_OFF = SQX_OFF + SQX_BYTES;
   static constexpr int SQY_BYTES = 2 * 3 * (TY + 2) * TX * 4;
   static constexpr int BAR_OFF = round_up_c(SQY_OFF + SQY_BYTES, 8);
-  static constexpr int SMEM = BAR_OFF + NB * 8;
+  // decoupled form (AS): "q rows of plane k published" (2, one per q slot) and "step k done"
+  // (DIST+1) barriers, an abort flag, and one producer warp beyond the NT compute lanes
+  static constexpr int NQP = AS ? 2 : 0, NFR = AS ? DIST + 1 : 0;
+  static constexpr int ABORT_OFF = BAR_OFF + (NB + NQP + NFR) * 8;
+  static constexpr int SMEM = ABORT_OFF + (AS ? 8 : 0);
+  static constexpr int NT_LAUNCH = NT + (AS ? 32 : 0);
 };
 
-template <typename SU, typename SP, int TX, int TY, int DIST, int V, int MINB, bool GEN>
-__global__ void __launch_bounds__(SplitGeom<SU, SP, TX, TY, DIST, V>::NT, MINB)
+template <typename SU, typename SP, int TX, int TY, int DIST, int V, int MINB, bool GEN, bool AS = false>
+__global__ void __launch_bounds__(SplitGeom<SU, SP, TX, TY, DIST, V, AS>::NT_LAUNCH, MINB)
 iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs,
                      const TMaps* __restrict__ maps, IterArgs a, int* __restrict__ status) {
-  using G = SplitGeom<SU, SP, TX, TY, DIST, V>;
+  using G = SplitGeom<SU, SP, TX, TY, DIST, V, AS>;
   using B = typename G::B;
   using T = LaneT<V>;
   constexpr int AU = B::AU, AP = B::AP, UXB = B::UXB, PXB = B::PXB;
@@ -776,16 +799,50 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
   // with zero stencil coefficients: they must hold zeros (0 * NaN = NaN)
   for (int i = tid; i < (G::SQX_BYTES + G::SQY_BYTES) / 4; i += blockDim.x)
     reinterpret_cast<float*>(smem + G::SQX_OFF)[i] = 0.f;
+  uint64_t* qpub = bars + G::NB;             // AS: q rows of plane k published, slot (k-kb) & 1
+  uint64_t* freed = qpub + G::NQP;           // AS: step k done by every lane, slot (k-kb) % NFR
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + G::ABORT_OFF);
   if (tid == 0) {
     for (int s = 0; s < G::NB; ++s) mbar_init(bars + s, 1);
+    if constexpr (AS) {
+      for (int s = 0; s < G::NQP; ++s) mbar_init(qpub + s, G::NT);
+      for (int s = 0; s < G::NFR; ++s) mbar_init(freed + s, G::NT);
+      *abort_flag = 0;
+    }
     mbar_fence_init();
   }
   __syncthreads();
   int issued = pl - 1;
-  if (tid == 0) {
-    const int last = min(kb + DIST - 1, ph);
-    for (int q = pl; q <= last; ++q) issue(q);
-    issued = last;
+  if constexpr (AS) {
+    // producer warp: issues every plane once the step that frees its slots is done
+    if (tid >= G::NT) {
+      if (tid == G::NT) {
+        const int last = min(kb + DIST - 1, ph);
+        for (int q = pl; q <= last; ++q) issue(q);
+        issued = last;
+        for (int q = kb + DIST; q <= ph; ++q) {
+          const int st = q - DIST - kb;
+          if (!mbar_wait_abort(freed + st % G::NFR, (uint32_t)((st / G::NFR) & 1), abort_flag)) break;
+          issue(q);
+          issued = q;
+        }
+        if (*abort_flag) {
+          atomicOr(status, SVS_DEV_TIMEOUT);
+          // wait (bounded) for the copies still in flight before the CTA may exit
+          for (int q = max(issued - G::NB + 1, pl); q <= issued; ++q) {
+            const int r = q - pl;
+            mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1));
+          }
+        }
+      }
+      return;
+    }
+  } else {
+    if (tid == 0) {
+      const int last = min(kb + DIST - 1, ph);
+      for (int q = pl; q <= last; ++q) issue(q);
+      issued = last;
+    }
   }
   int waited = pl - 1;
   bool bad = false;
@@ -796,7 +853,7 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
   for (int c = 0; c < 3; ++c) qmm[c] = qm[c] = qc[c] = bcast<T>(0.f);
   const float wtv2 = a.wtv * a.wtv;
 
-  // x/y part of the divergence at plane j (q rows of slot j & 1), loaded before the dual
+  // x/y part of the divergence at plane j (q rows of slot j & 1)
   auto load_dxy = [&](int j, T (&dxy)[3]) {
     const int ps = j & 1;
 #pragma unroll
@@ -833,6 +890,15 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
       for (int c = 0; c < 3; ++c) Store<SU>::st(dst + c * cs, first(n[c]));
     }
   };
+  // AS: waits on "q rows of plane j published" and "step j done by every lane"
+  auto wait_q = [&](int j) {
+    const int r = j - kb;
+    return mbar_wait_abort(qpub + (r & 1), (uint32_t)((r >> 1) & 1), abort_flag);
+  };
+  auto wait_free = [&](int j) {
+    const int r = j - kb;
+    return mbar_wait_abort(freed + r % G::NFR, (uint32_t)((r / G::NFR) & 1), abort_flag);
+  };
 
   // One plane step; WITH_PRIMAL: role 0 also finishes plane k-1.
   auto step = [&](const int k, auto with_primal) {
@@ -841,8 +907,11 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
     while (waited < need && !bad) {
       ++waited;
       const int r = waited - pl;
-      if (!mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1))) bad = true;
+      const bool ok = AS ? mbar_wait_abort(bars + r % G::NB, (uint32_t)((r / G::NB) & 1), abort_flag)
+                         : mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1));
+      if (!ok) bad = true;
     }
+    if (AS && bad) return;
     const int qs = k & 1;
     const SU* Uk = ubox(k) + uo;
     const unsigned char* PD = smem + G::PD_OFF + ((k - kb) % G::NPD) * B::PD_SLOT;
@@ -851,14 +920,21 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
     // coefficient for them is zero (every boundary type): plane k stands in for them
     const SU* Um = ubox(k - 1 >= pl ? k - 1 : k) + uo;
     const SU* Up = ubox(k + 1 <= ph ? k + 1 : k) + uo;
+    T dxy[3], um[3], qxo[3], qyo[3];
+    float qxs[3];
+    if (WP && role == 0) {
+      if (AS && !wait_q(k - 1)) {
+        bad = true;
+        return;
+      }
+      if (active && !bad) load_dxy(k - 1, dxy);
+    }
     if (role != 2) {
       if (active && !bad) {
         const StencilV<T> fz = bcast_st<T>(fz1);
-        T dxy[3];
-        if (WP && role == 0) load_dxy(k - 1, dxy);
         const SP* P = reinterpret_cast<const SP*>(PD) + po;
         const SP* Dm = reinterpret_cast<const SP*>(PD + B::P_SLOT) + po;
-        T pk[9], Dk[6], um[3];
+        T pk[9], Dk[6];
 #pragma unroll
         for (int c = 0; c < 9; ++c) pk[c] = Lane<V, SP>::ld(P + c * PC);
 #pragma unroll
@@ -873,30 +949,23 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
           const T ez = apply3<GEN>(fz, um[c], o, Lane<V, SU>::ld(Up + c * UC));
           dual_row(Dk, ex, ey, ez, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2], a.sigma, a.wtv, wtv2);
         }
-        if (role == 0) {
-          if (k >= z0 && k < z1) {
-            SP* dst = p_dst + (long long)k * plane;
-            if (full) {
+        if (role == 0 && k >= z0 && k < z1) {
+          SP* dst = p_dst + (long long)k * plane;
+          if (full) {
 #pragma unroll
-              for (int c = 0; c < 9; ++c) Lane<V, SP>::st(dst + c * cs, pk[c]);
-            } else {
+            for (int c = 0; c < 9; ++c) Lane<V, SP>::st(dst + c * cs, pk[c]);
+          } else {
 #pragma unroll
-              for (int c = 0; c < 9; ++c) Store<SP>::st(dst + c * cs, first(pk[c]));
-            }
+            for (int c = 0; c < 9; ++c) Store<SP>::st(dst + c * cs, first(pk[c]));
           }
+        }
 #pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const T* pc = &pk[3 * c];
-            Lane<V, float>::st(&sqx[qs][c][ly][lx + 2], dot3(Dk[0], Dk[1], Dk[2], pc[0], pc[1], pc[2]));
-            Lane<V, float>::st(&sqy[qs][c][ly + 1][lx], dot3(Dk[1], Dk[3], Dk[4], pc[0], pc[1], pc[2]));
+        for (int c = 0; c < 3; ++c) {
+          const T* pc = &pk[3 * c];
+          qyo[c] = dot3(Dk[1], Dk[3], Dk[4], pc[0], pc[1], pc[2]);
+          if (role == 0) {
+            qxo[c] = dot3(Dk[0], Dk[1], Dk[2], pc[0], pc[1], pc[2]);
             qc[c] = dot3(Dk[2], Dk[4], Dk[5], pc[0], pc[1], pc[2]);
-          }
-          if (WP) finish_primal(k - 1, dxy, qc, um);
-        } else {
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const T* pc = &pk[3 * c];
-            Lane<V, float>::st(&sqy[qs][c][ly + 1][lx], dot3(Dk[1], Dk[3], Dk[4], pc[0], pc[1], pc[2]));
           }
         }
       }
@@ -919,17 +988,39 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
         dual_row(Dk, ex, ey, ez, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2], a.sigma, a.wtv, wtv2);
       }
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
-        sqx[qs][c][ly][lx + 2] = dot3(Dk[0], Dk[1], Dk[2], pk[3 * c], pk[3 * c + 1], pk[3 * c + 2]);
+      for (int c = 0; c < 3; ++c) qxs[c] = dot3(Dk[0], Dk[1], Dk[2], pk[3 * c], pk[3 * c + 1], pk[3 * c + 2]);
     }
-    // everyone is done with plane k's p/D, plane k-1's u and rc/gw, and q rows of plane k-1
-    if (__syncthreads_or(bad)) {
+    // AS: the q slot of plane k was last read by the primal of plane k-2 (step k-1)
+    if (AS && k > kb && !wait_free(k - 1)) {
       bad = true;
       return;
     }
-    if (tid == 0 && k + DIST <= ph && k + DIST > issued) {
-      issue(k + DIST);
-      issued = k + DIST;
+    if (active && !bad) {
+      if (role == 2) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sqx[qs][c][ly][lx + 2] = qxs[c];
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          Lane<V, float>::st(&sqy[qs][c][ly + 1][lx], qyo[c]);
+          if (role == 0) Lane<V, float>::st(&sqx[qs][c][ly][lx + 2], qxo[c]);
+        }
+      }
+    }
+    if constexpr (AS) mbar_arrive(qpub + ((k - kb) & 1));
+    if (WP && role == 0 && active && !bad) finish_primal(k - 1, dxy, qc, um);
+    if constexpr (AS) {
+      mbar_arrive(freed + (k - kb) % G::NFR);
+    } else {
+      // everyone is done with plane k's p/D, plane k-1's u and rc/gw, and q rows of plane k-1
+      if (__syncthreads_or(bad)) {
+        bad = true;
+        return;
+      }
+      if (tid == 0 && k + DIST <= ph && k + DIST > issued) {
+        issue(k + DIST);
+        issued = k + DIST;
+      }
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -944,7 +1035,10 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
   for (; k < kp && !bad; ++k) step(k, std::false_type{});
   for (; k <= ke && !bad; ++k) step(k, std::true_type{});
   if (bad) {
-    if (tid == 0) {
+    if constexpr (AS) {
+      *abort_flag = 1;
+      atomicOr(status, SVS_DEV_TIMEOUT);
+    } else if (tid == 0) {
       atomicOr(status, SVS_DEV_TIMEOUT);
       // wait (bounded) for the copies this CTA still has in flight before it exits
       for (int q = max(waited + 1, pl); q <= issued; ++q) {
@@ -956,6 +1050,10 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
   }
   if (z1 >= nz) {
     const int j = nz - 1;
+    if (AS && role == 0 && !wait_q(j)) {
+      atomicOr(status, SVS_DEV_TIMEOUT);
+      return;
+    }
     if (role == 0 && active && j >= z0) {
       T dxy[3], uj[3];
       const T zero[3] = {bcast<T>(0.f), bcast<T>(0.f), bcast<T>(0.f)};
@@ -971,11 +1069,13 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
 // the register budget is sized for); instantiated in svs_split.cu.
 struct SplitShape {
   int tx, ty, dist, v, minb;
+  bool as;  // decoupled synchronisation (mbarriers and a producer warp instead of __syncthreads)
 };
 constexpr SplitShape kSplitShapes[] = {
-    {32, 8, 3, 2, 1},  {32, 8, 4, 2, 1}, {16, 16, 3, 2, 1}, {40, 8, 3, 2, 2}, {32, 16, 3, 2, 1},
-    {40, 16, 3, 2, 1}, {32, 8, 3, 1, 2}, {32, 8, 4, 1, 2},  {16, 16, 3, 1, 2}, {32, 16, 2, 1, 1},
-    {32, 16, 3, 1, 1}, {40, 8, 3, 1, 2}};
+    {32, 8, 3, 2, 1, false},  {32, 8, 4, 2, 1, false},  {16, 16, 3, 2, 1, false}, {40, 8, 3, 2, 2, false},
+    {32, 16, 3, 2, 1, false}, {40, 16, 3, 2, 1, false}, {32, 8, 3, 1, 2, false},  {32, 8, 4, 1, 2, false},
+    {16, 16, 3, 1, 2, false}, {32, 16, 2, 1, 1, false}, {32, 16, 3, 1, 1, false}, {40, 8, 3, 1, 2, false},
+    {40, 8, 3, 2, 2, true},   {32, 8, 3, 2, 2, true},   {16, 16, 3, 1, 2, true},  {32, 16, 3, 2, 1, true}};
 constexpr int kNumSplitShapes = sizeof(kSplitShapes) / sizeof(kSplitShapes[0]);
 
 // Split-role variant `idx` for a storage mode. op 0: set the kernels' shared-memory attribute

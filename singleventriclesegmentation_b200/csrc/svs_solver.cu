@@ -50,7 +50,8 @@ constexpr TileShape kTileShapes[] = {
     {32, 16, 2, kTma, 0},  {32, 8, 0, kPlain, 0}, {32, 4, 0, kPlain, 0}, {16, 16, 0, kPlain, 0},
     split_entry(0),        split_entry(1),        split_entry(2),        split_entry(3),
     split_entry(4),        split_entry(5),        split_entry(6),        split_entry(7),
-    split_entry(8),        split_entry(9),        split_entry(10),       split_entry(11)};
+    split_entry(8),        split_entry(9),        split_entry(10),       split_entry(11),
+    split_entry(12),       split_entry(13),       split_entry(14),       split_entry(15)};
 constexpr bool split_table_complete() {
   int n = 0;
   for (const TileShape& t : kTileShapes) n += t.form == kSplit;
@@ -538,7 +539,8 @@ bool iter_dispatch(svs_plan& P, std::vector<TMaps>* maps, int level, int tid, in
 constexpr int split_id(int tx, int ty, int dist, int v) {
   for (int i = 0; i < kNumTileShapes; ++i)
     if (kTileShapes[i].form == kSplit && kTileShapes[i].tx == tx && kTileShapes[i].ty == ty &&
-        kTileShapes[i].dist == dist && kSplitShapes[kTileShapes[i].split].v == v)
+        kTileShapes[i].dist == dist && kSplitShapes[kTileShapes[i].split].v == v &&
+        !kSplitShapes[kTileShapes[i].split].as)
       return i + 1;
   return 0;
 }

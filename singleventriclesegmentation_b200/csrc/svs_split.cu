@@ -10,13 +10,13 @@ template <typename SU, typename SP, int I>
 bool run(int op, bool gen, unsigned nt, const Tile* tiles, const Desc* descs, const TMaps* maps,
          const IterArgs* a, int* status, cudaStream_t s, int* box) {
   constexpr SplitShape S = kSplitShapes[I];
-  using G = SplitGeom<SU, SP, S.tx, S.ty, S.dist, S.v>;
-  auto* kf = iterate_split_kernel<SU, SP, S.tx, S.ty, S.dist, S.v, S.minb, false>;
-  auto* kt = iterate_split_kernel<SU, SP, S.tx, S.ty, S.dist, S.v, S.minb, true>;
+  using G = SplitGeom<SU, SP, S.tx, S.ty, S.dist, S.v, S.as>;
+  auto* kf = iterate_split_kernel<SU, SP, S.tx, S.ty, S.dist, S.v, S.minb, false, S.as>;
+  auto* kt = iterate_split_kernel<SU, SP, S.tx, S.ty, S.dist, S.v, S.minb, true, S.as>;
   if (op == 2) {  // resident CTAs per SM (after op 0 set the shared-memory attribute)
     if (G::SMEM > 227 * 1024) return false;
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, gen ? kt : kf, G::NT, G::SMEM) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, gen ? kt : kf, G::NT_LAUNCH, G::SMEM) != cudaSuccess) {
       cudaGetLastError();
       return false;
     }
@@ -36,7 +36,7 @@ bool run(int op, bool gen, unsigned nt, const Tile* tiles, const Desc* descs, co
     box[3] = G::B::PYB;
     return true;
   }
-  (gen ? kt : kf)<<<nt, G::NT, G::SMEM, s>>>(tiles, descs, maps, *a, status);
+  (gen ? kt : kf)<<<nt, G::NT_LAUNCH, G::SMEM, s>>>(tiles, descs, maps, *a, status);
   return true;
 }
 
@@ -45,10 +45,11 @@ bool dispatch(int idx, int op, bool gen, unsigned nt, const Tile* tiles, const D
               const IterArgs* a, int* status, cudaStream_t s, int* box) {
 #define SVS_SPLIT(I) \
   case I: return run<SU, SP, I>(op, gen, nt, tiles, descs, maps, a, status, s, box);
-  static_assert(kNumSplitShapes == 12, "one case per compiled shape");
+  static_assert(kNumSplitShapes == 16, "one case per compiled shape");
   switch (idx) {
     SVS_SPLIT(0) SVS_SPLIT(1) SVS_SPLIT(2) SVS_SPLIT(3) SVS_SPLIT(4) SVS_SPLIT(5)
     SVS_SPLIT(6) SVS_SPLIT(7) SVS_SPLIT(8) SVS_SPLIT(9) SVS_SPLIT(10) SVS_SPLIT(11)
+    SVS_SPLIT(12) SVS_SPLIT(13) SVS_SPLIT(14) SVS_SPLIT(15)
     default: return false;
   }
 #undef SVS_SPLIT
