@@ -194,6 +194,19 @@ svs_status svs_tvl1_plan_set_tile(svs_plan* plan, int tile_id);
 /* Same for one pyramid level only (0 = fall back to the plan-wide choice). */
 svs_status svs_tvl1_plan_set_level_tile(svs_plan* plan, int level, int tile_id);
 int svs_tvl1_num_tiles(void);
+
+/* Residuals. With record != 0 every later solve logs, after each warp of each level, the
+ * root-mean-square change of each pair's flow over that warp, sqrt(sum (u_w - u_{w-1})^2 / 3N),
+ * reduced in FP64. With stop_tol > 0 a pair whose change falls below stop_tol skips the remaining
+ * warps of that level (its flow is final for the level); stop_tol > 0 needs an even
+ * max_outer_iterations. The reference computes per-iteration norms of the changes and never uses
+ * them (svs/modules/flow/tvl13d.py:240-253), always running every warp: record = 0 and
+ * stop_tol = 0 (the default) keep its schedule. Allocates the log and snapshot buffers. */
+svs_status svs_tvl1_plan_set_residuals(svs_plan* plan, int record, float stop_tol);
+/* Residual log of the last solve into out_host[(pair * levels + level) * max_warps + warp]
+ * (level 0 = finest; -1 where the warp was skipped); count = pairs * levels * max_warps.
+ * Synchronous. */
+svs_status svs_tvl1_plan_get_residuals(svs_plan* plan, float* out_host, size_t count);
 /* Shape of variant tile_id: tile width and height, prefetch distance, form (0 plain-load, 1 TMA
  * pipeline, 2 split-role TMA pipeline) and voxels per lane (1 or 2); any output may be NULL;
  * SVS_ERR_INVALID_ARG for an unknown id. No counterpart in the reference (a query for the

@@ -154,6 +154,7 @@ iterate_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs, I
 
   const Tile T = tiles[blockIdx.x];
   const Desc& Dg = descs[T.desc];
+  if (Dg.stop && *Dg.stop) return;  // pair converged for this level
   const int nz = Dg.nz, ny = Dg.ny, nx = Dg.nx;
   const int cs = (int)Dg.cs;
   const int plane = Dg.pitch * ny;
@@ -436,6 +437,7 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
 
   const Tile T = tiles[blockIdx.x];
   const Desc& Dg = descs[T.desc];
+  if (Dg.stop && *Dg.stop) return;  // pair converged for this level
   const TMaps* M = maps + T.desc;
   const int nz = Dg.nz, ny = Dg.ny, nx = Dg.nx;
   const int cs = (int)Dg.cs;
@@ -722,6 +724,7 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
 
   const Tile Tl = tiles[blockIdx.x];
   const Desc& Dg = descs[Tl.desc];
+  if (Dg.stop && *Dg.stop) return;  // pair converged for this level
   const TMaps* M = maps + Tl.desc;
   const int nz = Dg.nz, ny = Dg.ny, nx = Dg.nx;
   const int cs = (int)Dg.cs;

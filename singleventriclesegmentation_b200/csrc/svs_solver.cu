@@ -216,7 +216,7 @@ template <typename SU, typename SP>
 __global__ void linearise_kernel(const Desc* __restrict__ descs, int src, int interp, int bdry) {
   const Desc d = descs[blockIdx.y];
   const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (v >= d.n) return;
+  if (v >= d.n || (d.stop && *d.stop)) return;
   const int x = (int)(v % d.nx), y = (int)((v / d.nx) % d.ny), z = (int)(v / ((int64_t)d.nx * d.ny));
   const long long o = pidx(d, z, y, x);
   const SU* u = reinterpret_cast<const SU*>(d.u[src]);
@@ -315,6 +315,73 @@ __global__ void prolong_kernel(const Desc* __restrict__ coarse, const Desc* __re
 }
 
 // Level 0 planar state -> the caller's AoS layouts: u [Z,Y,X,3], p [Z,Y,X,3,3].
+// Residuals (optional): the root-mean-square change of each pair's flow over one warp,
+// sqrt(sum (u_w - u_{w-1})^2 / (3N)), summed in FP64 (warp shuffles, one atomic per block). The
+// reference computes per-iteration norms of the changes and never uses them (tvl13d.py:240-253);
+// here they are per warp and may stop a converged pair for the rest of the level.
+__global__ void residual_reset_kernel(int* __restrict__ stop, double* __restrict__ acc, int np) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < np) {
+    stop[i] = 0;
+    acc[i] = 0.0;
+  }
+}
+
+// snaps[pair] holds the flow at the end of the previous warp ([3][n] float); copy_only = 1 at
+// the start of a level takes the snapshot without accumulating.
+template <typename SU>
+__global__ void residual_kernel(const Desc* __restrict__ descs, int src, float* const* __restrict__ snaps,
+                                double* __restrict__ acc, int copy_only) {
+  const Desc d = descs[blockIdx.y];
+  if (*d.stop) return;  // uniform over the block
+  const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double sum = 0.0;
+  if (v < d.n) {
+    const int x = (int)(v % d.nx), y = (int)((v / d.nx) % d.ny), z = (int)(v / ((int64_t)d.nx * d.ny));
+    const long long o = pidx(d, z, y, x);
+    const SU* u = reinterpret_cast<const SU*>(d.u[src]);
+    float* snap = snaps[blockIdx.y];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float now = Store<SU>::ld(u + c * d.cs + o);
+      const double diff = (double)now - (double)snap[c * d.n + v];
+      sum += diff * diff;
+      snap[c * d.n + v] = now;
+    }
+  }
+  if (copy_only) return;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, off);
+  __shared__ double part[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) part[wid] = sum;
+  __syncthreads();
+  if (wid == 0) {
+    sum = lane < (int)(blockDim.x >> 5) ? part[lane] : 0.0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, off);
+    if (lane == 0) atomicAdd(acc + blockIdx.y, sum);
+  }
+}
+
+// Log the warp's residual of every pair (-1 if the pair had stopped) and apply the stop rule.
+__global__ void residual_finish_kernel(const Desc* __restrict__ descs, double* __restrict__ acc,
+                                       float* __restrict__ log, int levels, int warps, int level, int w,
+                                       float tol, int np) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const Desc& d = descs[i];
+  float* slot = log + ((size_t)i * levels + level) * warps + w;
+  if (*d.stop) {
+    *slot = -1.f;
+    return;
+  }
+  const double r = sqrt(acc[i] / (3.0 * (double)d.n));
+  *slot = (float)r;
+  acc[i] = 0.0;
+  if (tol > 0.f && r < (double)tol) *d.stop = 1;
+}
+
 template <typename SU, typename SP>
 __global__ void finalize_kernel(const Desc* __restrict__ descs, int src, float* const* __restrict__ u_out,
                                 float* const* __restrict__ p_out) {
@@ -394,6 +461,14 @@ struct svs_plan {
   int graph_tile = -1;
   bool graph_warm = false;
   bool graph_want_p = false;
+  // residuals (svs_tvl1_plan_set_residuals)
+  bool res_on = false;
+  float res_tol = 0.f;
+  int* d_stop = nullptr;                   // [pairs]
+  double* d_acc = nullptr;                 // [pairs]
+  float* d_reslog = nullptr;               // [pairs][levels][max_warps]
+  float** d_snaps = nullptr;               // [pairs] -> [3][n0] floats
+  std::vector<float*> snaps;
 };
 
 namespace svs {
@@ -698,6 +773,11 @@ long long enqueue_solve(svs_plan& P, cudaStream_t s) {
     const int zero = (l == L - 1) && !(P.warm && L == 1);
     prepare_kernel<SU, SP><<<grid(l), 256, 0, s>>>(D + (size_t)l * np, q.use_anisotropic_diff, q.alpha, q.beta, q.boundary, zero, cur);
     ++launches;
+    if (P.res_on) {
+      residual_reset_kernel<<<ceil_div(np, 128), 128, 0, s>>>(P.d_stop, P.d_acc, np);
+      residual_kernel<SU><<<grid(l), 256, 0, s>>>(D + (size_t)l * np, cur, P.d_snaps, P.d_acc, 1);
+      launches += 2;
+    }
     for (int w = 0; w < q.max_warps; ++w) {
       linearise_kernel<SU, SP><<<grid(l), 256, 0, s>>>(D + (size_t)l * np, cur, q.interpolation, q.boundary);
       ++launches;
@@ -706,6 +786,12 @@ long long enqueue_solve(svs_plan& P, cudaStream_t s) {
         iter_dispatch(P, nullptr, l, P.level_tile[l], 1, &a, s);
         ++launches;
         cur ^= 1;
+      }
+      if (P.res_on) {
+        residual_kernel<SU><<<grid(l), 256, 0, s>>>(D + (size_t)l * np, cur, P.d_snaps, P.d_acc, 0);
+        residual_finish_kernel<<<ceil_div(np, 128), 128, 0, s>>>(D + (size_t)l * np, P.d_acc, P.d_reslog, L,
+                                                                 q.max_warps, l, w, P.res_tol, np);
+        launches += 2;
       }
     }
     if (l > 0) {
@@ -917,6 +1003,11 @@ svs_status svs_tvl1_plan_destroy(svs_plan* P) {
   cudaFree(P->d_descs); cudaFree(P->d_raw); cudaFree(P->d_uout); cudaFree(P->d_umed);
   cudaFree(P->d_pout); cudaFree(P->d_uinit); cudaFree(P->d_pinit); cudaFree(P->d_maps);
   cudaFree(P->d_status);
+  cudaFree(P->d_stop);
+  cudaFree(P->d_acc);
+  cudaFree(P->d_reslog);
+  cudaFree(P->d_snaps);
+  for (float* p : P->snaps) cudaFree(p);
   cudaFree(P->arena);
   delete P;
   return SVS_OK;
@@ -940,6 +1031,48 @@ svs_status svs_tvl1_plan_set_level_tile(svs_plan* P, int level, int tile_id) {
   P->level_tile_req[level] = tile_id;
   ++P->tile_epoch;
   return SVS_OK;
+}
+
+svs_status svs_tvl1_plan_set_residuals(svs_plan* P, int record, float stop_tol) {
+  SVS_REQUIRE(P, "svs_tvl1_plan_set_residuals: null plan");
+  SVS_REQUIRE(stop_tol >= 0.f, "svs_tvl1_plan_set_residuals: stop_tol must be >= 0");
+  SVS_REQUIRE(stop_tol == 0.f || P->prm.max_outer_iterations % 2 == 0,
+              "svs_tvl1_plan_set_residuals: stopping needs an even max_outer_iterations (the iteration "
+              "state alternates between two buffers)");
+  const bool on = record != 0 || stop_tol > 0.f;
+  const int np = P->num_pairs;
+  if (on && !P->d_stop) {
+    svs_status st = check_cuda(cudaMalloc(&P->d_stop, np * sizeof(int)), "residuals");
+    if (!st) st = check_cuda(cudaMalloc(&P->d_acc, np * sizeof(double)), "residuals");
+    const size_t nlog = (size_t)np * P->levels * std::max(1, P->prm.max_warps);
+    if (!st) st = check_cuda(cudaMalloc(&P->d_reslog, nlog * sizeof(float)), "residuals");
+    if (!st) st = check_cuda(cudaMemset(P->d_reslog, 0, nlog * sizeof(float)), "residuals");
+    if (!st) st = check_cuda(cudaMemset(P->d_stop, 0, np * sizeof(int)), "residuals");
+    P->snaps.assign(np, nullptr);
+    for (int i = 0; i < np && !st; ++i)
+      st = check_cuda(cudaMalloc(&P->snaps[i], 3 * (size_t)P->h_descs[i].n * sizeof(float)), "residuals");
+    if (!st) st = check_cuda(cudaMalloc(&P->d_snaps, np * sizeof(float*)), "residuals");
+    if (!st) st = check_cuda(cudaMemcpy(P->d_snaps, P->snaps.data(), np * sizeof(float*), cudaMemcpyHostToDevice), "residuals");
+    if (st) return st;
+  }
+  // the flag pointer in every descriptor (null when off: the kernels test it)
+  for (int l = 0; l < P->levels; ++l)
+    for (int i = 0; i < np; ++i) P->h_descs[(size_t)l * np + i].stop = on ? P->d_stop + i : nullptr;
+  svs_status st = check_cuda(cudaMemcpy(P->d_descs, P->h_descs.data(), P->h_descs.size() * sizeof(Desc),
+                                        cudaMemcpyHostToDevice), "residuals");
+  if (st) return st;
+  P->res_on = on;
+  P->res_tol = stop_tol;
+  ++P->tile_epoch;  // the captured graph changes
+  return SVS_OK;
+}
+
+svs_status svs_tvl1_plan_get_residuals(svs_plan* P, float* out, size_t count) {
+  SVS_REQUIRE(P && out, "svs_tvl1_plan_get_residuals: null pointer");
+  SVS_REQUIRE(P->d_reslog, "svs_tvl1_plan_get_residuals: residuals are not recorded (svs_tvl1_plan_set_residuals)");
+  const size_t nlog = (size_t)P->num_pairs * P->levels * std::max(1, P->prm.max_warps);
+  SVS_REQUIRE(count == nlog, "svs_tvl1_plan_get_residuals: count must be pairs x levels x max_warps");
+  return check_cuda(cudaMemcpy(out, P->d_reslog, nlog * sizeof(float), cudaMemcpyDeviceToHost), "residuals");
 }
 
 svs_status svs_tvl1_solve_batch(svs_plan* P, const svs_pair_desc* pairs, int num_pairs,

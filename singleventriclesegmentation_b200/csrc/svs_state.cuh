@@ -74,6 +74,7 @@ struct Desc {
   void* gw;
   void* u[2];
   void* p[2];
+  int* stop;  // optional per-pair flag (residual stopping): non-zero = skip the rest of the level
 };
 
 __device__ __forceinline__ long long pidx(const Desc& d, int z, int y, int x) {

@@ -14,6 +14,7 @@ import ctypes
 import math
 from typing import List, Literal, Optional, Sequence, Tuple
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -28,6 +29,7 @@ class SolverPlan:
     def __init__(self, params: TVL1Params, dims: Sequence[Tuple[int, int, int]], device: torch.device):
         self.dims = [tuple(int(v) for v in d) for d in dims]
         self.device = device
+        self.params = params
         arr = (ctypes.c_int * (3 * len(self.dims)))(*[v for d in self.dims for v in d])
         handle = ctypes.c_void_p()
         with torch.cuda.device(device):
@@ -73,6 +75,22 @@ class SolverPlan:
 
     def level_tiles(self):
         return [int(_lib.lib().svs_tvl1_plan_level_tile(self._h, l)) for l in range(8)]
+
+    def set_residuals(self, record: bool = True, stop_tol: float = 0.0) -> None:
+        """Log the per-warp RMS change of each pair's flow (FP64 reduction) and, with stop_tol > 0,
+        skip the remaining warps of a level once a pair's change falls below stop_tol."""
+        with torch.cuda.device(self.device):
+            check(_lib.lib().svs_tvl1_plan_set_residuals(self._h, int(bool(record)), float(stop_tol)))
+        self._res_shape = (len(self.dims), self.params.num_scales, max(1, self.params.max_warps))
+
+    def residuals(self) -> np.ndarray:
+        """[pairs, levels, warps] log of the last solve (level 0 = finest, -1 = warp skipped)."""
+        shape = getattr(self, "_res_shape", None)
+        if shape is None:
+            raise RuntimeError("residuals are not recorded (call set_residuals first)")
+        out = np.empty(shape, dtype=np.float32)
+        check(_lib.lib().svs_tvl1_plan_get_residuals(self._h, out.ctypes.data, out.size))
+        return out
 
     @property
     def graph_kernels(self) -> int:
