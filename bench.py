@@ -211,13 +211,13 @@ def config_dict(args, storage):
 
 
 # ------------------------------------------------------------------------ shared helpers
-def tune_plan(plan, storage: str, levels: int = 3):
-    """Pick the fastest iterate-kernel variant per pyramid level on the plan's own state
-    (TMA and split-role forms)."""
+def tune_plan(plan, storage: str, levels: int = 3, per_class: bool = False):
+    """Pick the fastest iterate-kernel variant per pyramid level on the plan's own state (TMA
+    and split-role forms); with per_class also per size class of each level."""
     from singleventriclesegmentation_b200 import _lib, autotune
     n = int(_lib.lib().svs_tvl1_num_tiles())
     cands = [t for t in range(1, n + 1) if _lib.tile_info(t)["form"] != "plain"]
-    return autotune.tune(plan, storage, levels, candidates=cands, use_cache=False, iters=6)
+    return autotune.tune(plan, storage, levels, candidates=cands, use_cache=False, iters=6, per_class=per_class)
 
 
 def iterate_roofline(plan, storage: str, level_voxels: int, stream, dev):
@@ -310,7 +310,7 @@ def run_uneven(args):
     outs = [torch.empty(d + (3,), device=dev) for d in dims]
     solver = _solver(dev, args.storage)
     plan = solver.plan_for(dims)
-    tiles = None if args.no_autotune else tune_plan(plan, args.storage)
+    tiles = None if args.no_autotune else tune_plan(plan, args.storage, per_class=True)
     ms, clocks = _timed_solves(plan, I0s, I1s, outs, args.steps, args.warmup, dev)
     vox = sum(int(np.prod(d)) for d in dims)
     it_ms, alg = iterate_roofline(plan, args.storage, vox, torch.cuda.current_stream(dev), dev)
@@ -321,7 +321,9 @@ def run_uneven(args):
         "higher_is_better": True, "equivalent_80cube_pairs_per_s": vox / 512000.0 / (ms / 1000.0),
         "dtype": f"f32 math, {args.storage} storage", "data": "synthetic",
         "config": {"workload": "64 pairs, dims per axis uniform on {40,48,...,128} (seed 3), one batched solve",
-                   "total_voxels": vox, "storage": args.storage, "level_tiles": plan.level_tiles()[:3]},
+                   "total_voxels": vox, "storage": args.storage, "level_tiles": plan.level_tiles()[:3],
+                   "class_tiles": {str(l): {str(w): t for w, t in c.items()}
+                                   for l, c in getattr(plan, "class_tiles", {}).items()}},
         "roofline": {"bound": "hbm", "achieved": alg / (it_ms / 1000.0) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": alg / (it_ms / 1000.0) / 1e9 / peak, "peak_kind": kind, "launch_ms": it_ms},
         "clocks": clocks}), flush=True)

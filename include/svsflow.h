@@ -193,6 +193,10 @@ size_t svs_tvl1_plan_device_bytes(const svs_plan* plan);
 svs_status svs_tvl1_plan_set_tile(svs_plan* plan, int tile_id);
 /* Same for one pyramid level only (0 = fall back to the plan-wide choice). */
 svs_status svs_tvl1_plan_set_level_tile(svs_plan* plan, int level, int tile_id);
+/* Same for one pair at one level (0 = the level's variant). Pairs of a level that ask for another
+ * variant than the level's form a group per variant; the groups run concurrently (parallel
+ * branches of the solve's graph). Used by the autotuner to pick variants per size class. */
+svs_status svs_tvl1_plan_set_pair_tile(svs_plan* plan, int level, int pair, int tile_id);
 int svs_tvl1_num_tiles(void);
 
 /* Residuals. With record != 0 every later solve logs, after each warp of each level, the

@@ -80,9 +80,67 @@ def time_variant(plan: SolverPlan, level: int, tile: int, iters: int = 6) -> Opt
     return e0.elapsed_time(e1) / iters
 
 
+def time_level(plan: SolverPlan, level: int, iters: int = 6) -> Optional[float]:
+    """Mean milliseconds per iteration of `level` with the plan's current variant assignment
+    (all groups of pairs), or None if an assigned variant does not fit."""
+    try:
+        plan.bench_iterations(level, 2)
+    except _lib.SVSError as e:
+        if e.status == 5:
+            return None
+        raise
+    torch.cuda.synchronize(plan.device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    plan.bench_iterations(level, iters)
+    e1.record()
+    torch.cuda.synchronize(plan.device)
+    return e0.elapsed_time(e1) / iters
+
+
+def _pair_level_dims(dims, level: int):
+    out = []
+    for d in dims:
+        d = tuple(d)
+        for _ in range(level):
+            d = tuple((v + 1) // 2 for v in d)
+        out.append(d)
+    return out
+
+
+def tune_classes(plan: SolverPlan, level: int, candidates: Sequence[int], iters: int = 6) -> Dict[int, int]:
+    """Per size class of a level (pairs of equal width at that level): try `candidates` for the
+    class's pairs while the others keep their variant, timing the whole level (the groups run
+    concurrently), and keep a class's choice when it is at least 2% faster. Returns
+    {width: tile id} for the classes that left the level's variant."""
+    ld = _pair_level_dims(plan.dims, level)
+    widths = sorted({d[2] for d in ld})
+    if len(widths) < 2:
+        return {}
+    base = time_level(plan, level, iters)
+    chosen = {}
+    for w in widths:
+        members = [i for i, d in enumerate(ld) if d[2] == w]
+        best_t, best_tid = base, 0
+        for t in candidates:
+            for i in members:
+                plan.set_pair_tile(level, i, t)
+            ms = time_level(plan, level, iters)
+            if ms is not None and ms < best_t * 0.98:
+                best_t, best_tid = ms, t
+        for i in members:
+            plan.set_pair_tile(level, i, best_tid)
+        base = best_t
+        if best_tid:
+            chosen[w] = best_tid
+    return chosen
+
+
 def tune(plan: SolverPlan, storage: str, levels: int, candidates: Optional[Sequence[int]] = None,
-         use_cache: bool = True, iters: int = 6) -> List[int]:
-    """Choose and set the fastest variant per level; returns the chosen ids (level 0 first)."""
+         use_cache: bool = True, iters: int = 6, per_class: bool = False, class_candidates: int = 3) -> List[int]:
+    """Choose and set the fastest variant per level; returns the chosen ids (level 0 first).
+    With per_class, then let each size class of a level take one of the level's
+    `class_candidates` fastest variants (tune_classes)."""
     candidates = list(candidates or range(1, int(_lib.lib().svs_tvl1_num_tiles()) + 1))
     db = _load() if use_cache else {}
     chosen = []
@@ -90,13 +148,20 @@ def tune(plan: SolverPlan, storage: str, levels: int, candidates: Optional[Seque
     for level in range(levels):
         key = _key(plan.device, storage, [lds[level]])
         best = db.get(key)
-        if best is None:
+        ranked = None
+        if best is None or per_class:
             timings = {t: time_variant(plan, level, t, iters) for t in candidates}
             timings = {t: v for t, v in timings.items() if v is not None}
-            best = min(timings, key=timings.get)
+            ranked = sorted(timings, key=timings.get)
+            best = ranked[0] if best is None else best
             db[key] = best
         plan.set_level_tile(level, best)
         chosen.append(best)
+        if per_class and ranked:
+            cls = tune_classes(plan, level, [t for t in ranked[:class_candidates + 1] if t != best][:class_candidates],
+                               iters)
+            plan.class_tiles = getattr(plan, "class_tiles", {})
+            plan.class_tiles[level] = cls
     if use_cache:
         _store(db)
     return chosen

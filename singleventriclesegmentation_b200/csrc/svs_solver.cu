@@ -461,6 +461,21 @@ struct svs_plan {
   int graph_tile = -1;
   bool graph_warm = false;
   bool graph_want_p = false;
+  // pairs whose variant differs from their level's (svs_tvl1_plan_set_pair_tile): per level, one
+  // group per variant; the groups of a level run as parallel branches of the graph
+  struct TileGroup {
+    int tid = 0;
+    std::vector<svs::Tile> h;
+    svs::Tile* d = nullptr;
+  };
+  std::vector<std::vector<TileGroup>> extra;  // [level]
+  std::vector<std::vector<int>> pair_tile_req;  // [level][pair], 0 = the level's variant
+  const std::vector<char>* pair_mask = nullptr; // during set-up: the pairs a dispatch or tile build covers
+  const svs::Tile* launch_tiles = nullptr;      // launch override (a group's tiles)
+  unsigned launch_count = 0;
+  bool launch_override = false;
+  std::vector<cudaStream_t> side;               // one per group of the widest level
+  std::vector<cudaEvent_t> events;              // fork + one join per side stream
   // residuals (svs_tvl1_plan_set_residuals)
   bool res_on = false;
   float res_tol = 0.f;
@@ -521,6 +536,7 @@ bool encode_maps(svs_plan& P, std::vector<TMaps>& maps, int level, int ux, int u
   const bool bf = is_bf16(P.prm.storage);
   const int esu = (int)flow_bytes(P.prm.storage), esp = (int)field_bytes(P.prm.storage);
   for (int i = 0; i < P.num_pairs; ++i) {
+    if (P.pair_mask && !(*P.pair_mask)[i]) continue;
     const size_t k = (size_t)level * P.num_pairs + i;
     const Desc& d = P.h_descs[k];
     TMaps& m = maps[k];
@@ -554,8 +570,9 @@ bool tma_prepare(svs_plan& P, std::vector<TMaps>& maps, int level) {
 template <typename SU, typename SP>
 bool iter_variant(svs_plan& P, std::vector<TMaps>* maps, int level, int tid, int op, const IterArgs* a,
                   cudaStream_t s) {
-  const unsigned nt = (unsigned)P.h_tiles[level].size();
-  const Tile* tl = P.d_tiles.empty() ? nullptr : P.d_tiles[level];
+  const unsigned nt = P.launch_override ? P.launch_count : (unsigned)P.h_tiles[level].size();
+  const Tile* tl = P.launch_override ? P.launch_tiles : (P.d_tiles.empty() ? nullptr : P.d_tiles[level]);
+  if (op == 1 && nt == 0) return true;  // nothing of this level runs this variant
   // the MIRROR boundary (the solver's default) gets two-term stencils; other boundaries the
   // general three-term form
   const bool gen = P.prm.boundary != SVS_BOUNDARY_MIRROR;
@@ -594,8 +611,9 @@ bool iter_dispatch(svs_plan& P, std::vector<TMaps>* maps, int level, int tid, in
                    cudaStream_t s) {
   const TileShape& ts = kTileShapes[tid - 1];
   if (ts.form == kSplit) {
-    const unsigned nt = (unsigned)P.h_tiles[level].size();
-    const Tile* tl = P.d_tiles.empty() ? nullptr : P.d_tiles[level];
+    const unsigned nt = P.launch_override ? P.launch_count : (unsigned)P.h_tiles[level].size();
+    const Tile* tl = P.launch_override ? P.launch_tiles : (P.d_tiles.empty() ? nullptr : P.d_tiles[level]);
+    if (op == 1 && nt == 0) return true;
     const bool gen = P.prm.boundary != SVS_BOUNDARY_MIRROR;
     int box[4] = {0, 0, 0, 0};
     if (!split_variant(P.prm.storage, ts.split, op, gen, nt, tl, P.d_descs, P.d_maps, a, P.d_status, s, box))
@@ -658,7 +676,8 @@ int split_chunks(const svs_plan& P, int level, int tid, long long xy_tiles) {
                      nullptr, nullptr, nullptr, nullptr, box))
     return 1;
   per_sm = std::max(1, box[0]);
-  for (int i = 0; i < P.num_pairs; ++i) nz = std::max(nz, P.h_descs[(size_t)level * P.num_pairs + i].nz);
+  for (int i = 0; i < P.num_pairs; ++i)
+    if (!P.pair_mask || (*P.pair_mask)[i]) nz = std::max(nz, P.h_descs[(size_t)level * P.num_pairs + i].nz);
   const long long slots = (long long)sms * per_sm;
   int best = 1;
   long long best_cost = -1;
@@ -673,12 +692,16 @@ int split_chunks(const svs_plan& P, int level, int tid, long long xy_tiles) {
   return best;
 }
 
-void build_tiles(svs_plan& P, int level, int tid) {
+// Tiles of the level's pairs (those in P.pair_mask when set) for variant tid, into `out_opt` or
+// the level's own list.
+void build_tiles(svs_plan& P, int level, int tid, std::vector<Tile>* out_opt = nullptr) {
   const TileShape ts = kTileShapes[tid - 1];
-  std::vector<Tile>& out = P.h_tiles[level];
+  std::vector<Tile>& out = out_opt ? *out_opt : P.h_tiles[level];
   out.clear();
+  auto in = [&](int i) { return !P.pair_mask || (*P.pair_mask)[i]; };
   long long xy_tiles = 0;
   for (int i = 0; i < P.num_pairs; ++i) {
+    if (!in(i)) continue;
     const Desc& d = P.h_descs[(size_t)level * P.num_pairs + i];
     xy_tiles += (long long)ceil_div(d.nx, ts.tx) * ceil_div(d.ny, ts.ty);
   }
@@ -687,6 +710,7 @@ void build_tiles(svs_plan& P, int level, int tid) {
   const int split_c = ts.form == kSplit ? split_chunks(P, level, tid, xy_tiles) : 0;
   const long long target = 148LL * 2;
   for (int i = 0; i < P.num_pairs; ++i) {
+    if (!in(i)) continue;
     const Desc& d = P.h_descs[(size_t)level * P.num_pairs + i];
     int chunks = 1;
     if (split_c > 0)
@@ -708,26 +732,78 @@ svs_status setup_tiles(svs_plan& P) {
   const int want = P.tile_id;
   P.h_tiles.assign(P.levels, {});
   P.level_tile.assign(P.levels, 0);
+  for (auto& lv : P.extra)
+    for (auto& grp : lv) cudaFree(grp.d);
+  P.extra.assign(P.levels, {});
   std::vector<TMaps> maps((size_t)P.levels * P.num_pairs);
   std::memset(maps.data(), 0, maps.size() * sizeof(TMaps));
   for (int l = 0; l < P.levels; ++l) {
     const int req = (l < (int)P.level_tile_req.size() && P.level_tile_req[l] > 0) ? P.level_tile_req[l] : want;
     int tid = req > 0 ? req : auto_tile(P, l);
+    // per-pair requests that differ from the level's variant form groups of their own
+    std::vector<int> own(P.num_pairs, 0);
+    if (l < (int)P.pair_tile_req.size())
+      for (int i = 0; i < P.num_pairs; ++i) own[i] = P.pair_tile_req[l][i];
+    std::vector<char> mask(P.num_pairs, 1);
+    for (int i = 0; i < P.num_pairs; ++i) mask[i] = own[i] == 0 || own[i] == tid;
+    P.pair_mask = &mask;
     // attributes and tensor maps first: the tile builder asks the occupancy calculator
     if (!iter_dispatch(P, &maps, l, tid, 0, nullptr, nullptr)) {
-      if (req > 0) return fail(SVS_ERR_UNSUPPORTED, "tile variant not usable for this plan (shared memory or TMA descriptor limits)");
+      if (req > 0) {
+        P.pair_mask = nullptr;
+        return fail(SVS_ERR_UNSUPPORTED, "tile variant not usable for this plan (shared memory or TMA descriptor limits)");
+      }
       tid = 6;  // plain-load 32x8
+      for (int i = 0; i < P.num_pairs; ++i) mask[i] = own[i] == 0 || own[i] == tid;
     }
     build_tiles(P, l, tid);
     P.level_tile[l] = tid;
+    for (int i = 0; i < P.num_pairs; ++i) {
+      if (mask[i]) continue;
+      const int g = own[i];
+      bool seen = false;
+      for (auto& grp : P.extra[l]) seen |= grp.tid == g;
+      if (seen) continue;
+      std::vector<char> gm(P.num_pairs, 0);
+      for (int j = 0; j < P.num_pairs; ++j) gm[j] = own[j] == g && !mask[j];
+      P.pair_mask = &gm;
+      if (!iter_dispatch(P, &maps, l, g, 0, nullptr, nullptr)) {
+        P.pair_mask = nullptr;
+        return fail(SVS_ERR_UNSUPPORTED, "pair tile variant not usable for this plan (shared memory or TMA descriptor limits)");
+      }
+      svs_plan::TileGroup grp;
+      grp.tid = g;
+      build_tiles(P, l, g, &grp.h);
+      P.extra[l].push_back(std::move(grp));
+    }
+    P.pair_mask = nullptr;
   }
   for (auto* p : P.d_tiles) cudaFree(p);
   P.d_tiles.assign(P.levels, nullptr);
+  size_t widest = 0;
   for (int l = 0; l < P.levels; ++l) {
     const size_t bytes = P.h_tiles[l].size() * sizeof(Tile);
-    svs_status st = check_cuda(cudaMalloc(&P.d_tiles[l], bytes), "tile list");
-    if (!st) st = check_cuda(cudaMemcpy(P.d_tiles[l], P.h_tiles[l].data(), bytes, cudaMemcpyHostToDevice), "tile list");
+    svs_status st = check_cuda(cudaMalloc(&P.d_tiles[l], std::max<size_t>(bytes, sizeof(Tile))), "tile list");
+    if (!st && bytes) st = check_cuda(cudaMemcpy(P.d_tiles[l], P.h_tiles[l].data(), bytes, cudaMemcpyHostToDevice), "tile list");
+    for (auto& grp : P.extra[l]) {
+      const size_t gb = grp.h.size() * sizeof(Tile);
+      if (!st) st = check_cuda(cudaMalloc(&grp.d, gb), "tile list");
+      if (!st) st = check_cuda(cudaMemcpy(grp.d, grp.h.data(), gb, cudaMemcpyHostToDevice), "tile list");
+    }
     if (st) return st;
+    widest = std::max(widest, P.extra[l].size());
+  }
+  while (P.side.size() < widest) {
+    cudaStream_t st_ = nullptr;
+    svs_status st = check_cuda(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "group stream");
+    if (st) return st;
+    P.side.push_back(st_);
+  }
+  while (P.events.size() < widest + 1) {
+    cudaEvent_t e = nullptr;
+    svs_status st = check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "group event");
+    if (st) return st;
+    P.events.push_back(e);
   }
   return check_cuda(cudaMemcpy(P.d_maps, maps.data(), maps.size() * sizeof(TMaps), cudaMemcpyHostToDevice), "tensor maps");
 }
@@ -747,6 +823,34 @@ IterArgs iter_args(const svs_plan& P, int it, int cur) {
   a.src = cur;
   a.bdry = P.prm.boundary;
   return a;
+}
+
+// Groups of pairs with their own variant (svs_tvl1_plan_set_pair_tile) run on side streams:
+// fork after the level's linearisation, one launch per group and iteration, join before the next.
+size_t level_groups(const svs_plan& P, int l) { return l < (int)P.extra.size() ? P.extra[l].size() : 0; }
+void fork_groups(svs_plan& P, int l, cudaStream_t s) {
+  if (!level_groups(P, l)) return;
+  cudaEventRecord(P.events[0], s);
+  for (size_t g = 0; g < level_groups(P, l); ++g) cudaStreamWaitEvent(P.side[g], P.events[0], 0);
+}
+void join_groups(svs_plan& P, int l, cudaStream_t s) {
+  for (size_t g = 0; g < level_groups(P, l); ++g) {
+    cudaEventRecord(P.events[1 + g], P.side[g]);
+    cudaStreamWaitEvent(s, P.events[1 + g], 0);
+  }
+}
+// One iteration of level l over all its pairs; returns the launches issued.
+int level_iteration(svs_plan& P, int l, const IterArgs& a, cudaStream_t s) {
+  iter_dispatch(P, nullptr, l, P.level_tile[l], 1, &a, s);
+  for (size_t g = 0; g < level_groups(P, l); ++g) {
+    const svs_plan::TileGroup& grp = P.extra[l][g];
+    P.launch_override = true;
+    P.launch_tiles = grp.d;
+    P.launch_count = (unsigned)grp.h.size();
+    iter_dispatch(P, nullptr, l, grp.tid, 1, &a, P.side[g]);
+    P.launch_override = false;
+  }
+  return 1 + (int)level_groups(P, l);
 }
 
 // The whole batched solve as a sequence of launches on stream s. Returns the number of kernel
@@ -781,12 +885,13 @@ long long enqueue_solve(svs_plan& P, cudaStream_t s) {
     for (int w = 0; w < q.max_warps; ++w) {
       linearise_kernel<SU, SP><<<grid(l), 256, 0, s>>>(D + (size_t)l * np, cur, q.interpolation, q.boundary);
       ++launches;
+      fork_groups(P, l, s);
       for (int it = 0; it < q.max_outer_iterations; ++it) {
         const IterArgs a = iter_args(P, it, cur);
-        iter_dispatch(P, nullptr, l, P.level_tile[l], 1, &a, s);
-        ++launches;
+        launches += level_iteration(P, l, a, s);
         cur ^= 1;
       }
+      join_groups(P, l, s);
       if (P.res_on) {
         residual_kernel<SU><<<grid(l), 256, 0, s>>>(D + (size_t)l * np, cur, P.d_snaps, P.d_acc, 0);
         residual_finish_kernel<<<ceil_div(np, 128), 128, 0, s>>>(D + (size_t)l * np, P.d_acc, P.d_reslog, L,
@@ -1003,6 +1108,10 @@ svs_status svs_tvl1_plan_destroy(svs_plan* P) {
   cudaFree(P->d_descs); cudaFree(P->d_raw); cudaFree(P->d_uout); cudaFree(P->d_umed);
   cudaFree(P->d_pout); cudaFree(P->d_uinit); cudaFree(P->d_pinit); cudaFree(P->d_maps);
   cudaFree(P->d_status);
+  for (auto& lv : P->extra)
+    for (auto& grp : lv) cudaFree(grp.d);
+  for (cudaStream_t st_ : P->side) cudaStreamDestroy(st_);
+  for (cudaEvent_t e : P->events) cudaEventDestroy(e);
   cudaFree(P->d_stop);
   cudaFree(P->d_acc);
   cudaFree(P->d_reslog);
@@ -1029,6 +1138,17 @@ svs_status svs_tvl1_plan_set_level_tile(svs_plan* P, int level, int tile_id) {
   SVS_REQUIRE(tile_id >= 0 && tile_id <= kNumTileShapes, "svs_tvl1_plan_set_level_tile: unknown tile id");
   if ((int)P->level_tile_req.size() < P->levels) P->level_tile_req.resize(P->levels, 0);
   P->level_tile_req[level] = tile_id;
+  ++P->tile_epoch;
+  return SVS_OK;
+}
+
+svs_status svs_tvl1_plan_set_pair_tile(svs_plan* P, int level, int pair, int tile_id) {
+  SVS_REQUIRE(P, "svs_tvl1_plan_set_pair_tile: null plan");
+  SVS_REQUIRE(level >= 0 && level < P->levels, "svs_tvl1_plan_set_pair_tile: bad level");
+  SVS_REQUIRE(pair >= 0 && pair < P->num_pairs, "svs_tvl1_plan_set_pair_tile: bad pair");
+  SVS_REQUIRE(tile_id >= 0 && tile_id <= kNumTileShapes, "svs_tvl1_plan_set_pair_tile: unknown tile id");
+  if ((int)P->pair_tile_req.size() < P->levels) P->pair_tile_req.resize(P->levels, std::vector<int>(P->num_pairs, 0));
+  P->pair_tile_req[level][pair] = tile_id;
   ++P->tile_epoch;
   return SVS_OK;
 }
@@ -1157,13 +1277,16 @@ svs_status svs_tvl1_bench_iterations(svs_plan* P, int level, int count, svs_stre
     P->tiles_built_for = P->tile_epoch;
   }
   int cur = 0;
+  uint64_t launches = 0;
+  fork_groups(*P, level, stream);
   for (int i = 0; i < count; ++i) {
     const int it = P->prm.max_outer_iterations > 0 ? i % P->prm.max_outer_iterations : 0;
     const IterArgs a = iter_args(*P, it, cur);
-    iter_dispatch(*P, nullptr, level, P->level_tile[level], 1, &a, stream);
+    launches += level_iteration(*P, level, a, stream);
     cur ^= 1;
   }
-  return check_launch("svs_tvl1_bench_iterations", (uint64_t)count);
+  join_groups(*P, level, stream);
+  return check_launch("svs_tvl1_bench_iterations", launches);
 }
 
 uint64_t svs_tvl1_plan_graph_kernels(const svs_plan* P) { return P ? P->graph_kernels : 0; }

@@ -76,6 +76,9 @@ class SolverPlan:
     def level_tiles(self):
         return [int(_lib.lib().svs_tvl1_plan_level_tile(self._h, l)) for l in range(8)]
 
+    def set_pair_tile(self, level: int, pair: int, tile_id: int) -> None:
+        check(_lib.lib().svs_tvl1_plan_set_pair_tile(self._h, int(level), int(pair), int(tile_id)))
+
     def set_residuals(self, record: bool = True, stop_tol: float = 0.0) -> None:
         """Log the per-warp RMS change of each pair's flow (FP64 reduction) and, with stop_tol > 0,
         skip the remaining warps of a level once a pair's change falls below stop_tol."""

@@ -159,6 +159,31 @@ def test_tile_variants_agree(cuda, storage, shape, over):
     assert e.mean() < 1e-4 and e.max() < 1e-2, (e.mean(), e.max())
 
 
+def test_pair_variant_groups_run_concurrently_with_the_same_result(cuda):
+    """Pairs given their own variants (svs_tvl1_plan_set_pair_tile) form groups that run as
+    parallel graph branches; TMA and split-role variants are bitwise equal, so the result of every
+    pair is unchanged."""
+    shapes = [(24, 24, 24), (21, 37, 45), (20, 40, 40)]
+    pairs = [synthetic.frame_pair(sh, seed=20 + i) for i, sh in enumerate(shapes)]
+    solver, _ = make_solver(storage="f16-flow32", max_warps=2, max_outer_iterations=20)
+    ref = solver.compute_batch([T(p[0]) for p in pairs], [T(p[1]) for p in pairs])
+    solver._plans.clear()
+    plan = solver.plan_for(shapes)
+    # level 0: pairs 1 and 2 on two other variants; level 1: pair 0 on another one
+    plan.set_pair_tile(0, 1, 17)
+    plan.set_pair_tile(0, 2, 12)
+    plan.set_pair_tile(1, 0, 9)
+    outs = [torch.empty(sh + (3,), device="cuda") for sh in shapes]
+    plan.solve([T(p[0]) for p in pairs], [T(p[1]) for p in pairs], outs)
+    torch.cuda.synchronize()
+    plan.check()
+    for a, b in zip(ref, outs):
+        assert torch.equal(a, b)
+    plan.bench_iterations(0, 4)   # the grouped level also runs outside the graph
+    torch.cuda.synchronize()
+    plan.check()
+
+
 def test_graph_reuse_and_new_inputs(cuda):
     solver, _ = make_solver(max_warps=2, max_outer_iterations=20)
     a = synthetic.frame_pair((16, 16, 16), seed=1)
