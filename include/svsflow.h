@@ -139,6 +139,38 @@ svs_status svs_gauss_blur3d(const float* in, int nz, int ny, int nx, const float
 svs_status svs_median3d(const float* in, int nz, int ny, int nx, int C, int ks, float* out,
                         svs_stream_t stream);
 
+/* FP64 forms of the per-operator entry points above: the same operators, arguments and
+ * semantics on double arrays, with double scalars (the reference dispatches float and double,
+ * AT_DISPATCH_FLOATING_TYPES in svs/src/*.cu). Used by the double-precision drop-in operators and
+ * the FP64 run of the plain solver on the GPU. */
+svs_status svs_nabla3d_forward_f64(const double* b, int nz, int ny, int nx, int C, double hz, double hy,
+                                   double hx, int boundary, double* out, svs_stream_t stream);
+svs_status svs_nabla3d_backward_f64(const double* p, int nz, int ny, int nx, int C, double hz, double hy,
+                                    double hx, int boundary, double* out, svs_stream_t stream);
+svs_status svs_aniso3d_tangents_f64(const double* g, int64_t n, double alpha, double beta, double* s,
+                                    double* normals, double* t1, double* t2, svs_stream_t stream);
+svs_status svs_aniso3d_apply_f64(const double* in, int64_t n, const double* s, const double* normals,
+                                 const double* t1, const double* t2, double* out, svs_stream_t stream);
+svs_status svs_tvl1_prox_primal_f64(const double* primal, int64_t n, double tau, double weight_matching,
+                                    const double* rho, const double* i1w_grad, double* out, svs_stream_t stream);
+svs_status svs_tvl1_prox_dual_f64(const double* dual, int64_t n, double sigma, double weight_tv, double* out,
+                                  svs_stream_t stream);
+svs_status svs_warp3d_f64(const double* u, int nz, int ny, int nx, int C, const double* phi, double hz,
+                          double hy, double hx, int interpolation, int boundary, double* out, svs_stream_t stream);
+svs_status svs_warp3d_backward_f64(const double* u, int nz, int ny, int nx, const double* phi,
+                                   const double* grad_out, double hz, double hy, double hx, int interpolation,
+                                   int boundary, double* grad_u, double* grad_phi, svs_stream_t stream);
+svs_status svs_warp_cnn3d_f64(const double* m, int B, int C, int nz, int ny, int nx, const double* phi,
+                              double hz, double hy, double hx, int interpolation, int boundary, double* out,
+                              svs_stream_t stream);
+svs_status svs_prolongate3d_f64(const double* u, int nz, int ny, int nx, int C, double lz, double ly,
+                                double lx, int tz, int ty, int tx, double tlz, double tly, double tlx,
+                                int interpolation, int boundary, double* out, svs_stream_t stream);
+svs_status svs_gauss_blur3d_f64(const double* in, int nz, int ny, int nx, const double* weights_host, int r,
+                                double* out, svs_stream_t stream);
+svs_status svs_median3d_f64(const double* in, int nz, int ny, int nx, int C, int ks, double* out,
+                            svs_stream_t stream);
+
 /* ---------------------------------------------------------------------------------------------
  * Fused solver: TVL13DOpticalFlow.compute (svs/modules/flow/tvl13d.py:122-162) for a batch of
  * independent frame pairs. Every pair is solved from zero flow at the coarsest level (the

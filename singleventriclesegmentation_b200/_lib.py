@@ -65,6 +65,18 @@ _SIGS = {
     "svs_prolongate3d": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_float, c_float, c_float, c_int, c_int, c_int, c_float, c_float, c_float, c_int, c_int, c_void_p, c_void_p]),
     "svs_gauss_blur3d": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p]),
     "svs_median3d": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p]),
+    "svs_nabla3d_forward_f64": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_double, c_double, c_double, c_int, c_void_p, c_void_p]),
+    "svs_nabla3d_backward_f64": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_double, c_double, c_double, c_int, c_void_p, c_void_p]),
+    "svs_aniso3d_tangents_f64": (c_int, [c_void_p, c_int64, c_double, c_double, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "svs_aniso3d_apply_f64": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "svs_tvl1_prox_primal_f64": (c_int, [c_void_p, c_int64, c_double, c_double, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "svs_tvl1_prox_dual_f64": (c_int, [c_void_p, c_int64, c_double, c_double, c_void_p, c_void_p]),
+    "svs_warp3d_f64": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_double, c_double, c_double, c_int, c_int, c_void_p, c_void_p]),
+    "svs_warp3d_backward_f64": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_double, c_double, c_double, c_int, c_int, c_void_p, c_void_p, c_void_p]),
+    "svs_warp_cnn3d_f64": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_double, c_double, c_double, c_int, c_int, c_void_p, c_void_p]),
+    "svs_prolongate3d_f64": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_double, c_double, c_double, c_int, c_int, c_int, c_double, c_double, c_double, c_int, c_int, c_void_p, c_void_p]),
+    "svs_gauss_blur3d_f64": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p]),
+    "svs_median3d_f64": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p]),
     "svs_tvl1_plan_create": (c_int, [ctypes.POINTER(TVL1Params), c_int, ctypes.POINTER(c_int), ctypes.POINTER(c_void_p)]),
     "svs_tvl1_plan_destroy": (c_int, [c_void_p]),
     "svs_tvl1_plan_device_bytes": (c_size_t, [c_void_p]),

@@ -9,31 +9,33 @@ namespace {
 
 constexpr int kMaxBlurTaps = 13 * 13 * 13;  // sigma up to 2.6 (kernel size int(5 sigma) made odd)
 
+template <typename T>
 struct BlurWeights {
-  float w[kMaxBlurTaps];
+  T w[kMaxBlurTaps];
 };
 
 // Zero-padded 3D correlation with a (2r+1)^3 kernel (F.conv3d, padding = r). Accumulates in
-// float in (z, y, x) tap order.
-__global__ void blur_kernel(const float* __restrict__ in, int nz, int ny, int nx, int r,
-                            const __grid_constant__ BlurWeights W, float* __restrict__ out) {
+// the value type in (z, y, x) tap order.
+template <typename T>
+__global__ void blur_kernel(const T* __restrict__ in, int nz, int ny, int nx, int r,
+                            const __grid_constant__ BlurWeights<T> W, T* __restrict__ out) {
   const int64_t n = (int64_t)nz * ny * nx;
   const int k = 2 * r + 1;
   for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n;
        v += (int64_t)gridDim.x * blockDim.x) {
     const int x = (int)(v % nx), y = (int)((v / nx) % ny), z = (int)(v / ((int64_t)nx * ny));
-    float acc = 0.f;
+    T acc = T(0);
     for (int a = 0; a < k; ++a) {
       const int zz = z + a - r;
       if (zz < 0 || zz >= nz) continue;
       for (int b = 0; b < k; ++b) {
         const int yy = y + b - r;
         if (yy < 0 || yy >= ny) continue;
-        const float* row = in + ((size_t)zz * ny + yy) * nx;
-        const float* wr = W.w + (a * k + b) * k;
+        const T* row = in + ((size_t)zz * ny + yy) * nx;
+        const T* wr = W.w + (a * k + b) * k;
         for (int c = 0; c < k; ++c) {
           const int xx = x + c - r;
-          if (xx >= 0 && xx < nx) acc = fmaf(wr[c], __ldg(row + xx), acc);
+          if (xx >= 0 && xx < nx) acc = fma(wr[c], __ldg(row + xx), acc);
         }
       }
     }
@@ -43,8 +45,9 @@ __global__ void blur_kernel(const float* __restrict__ in, int nz, int ny, int nx
 
 // Median of 27 by rank counting: the element with fewer than 14 smaller values and at least 14
 // values not larger than it (exact with ties, no sorting network state).
-__device__ __forceinline__ float median27(const float (&w)[27]) {
-  float med = w[0];
+template <typename T>
+__device__ __forceinline__ T median27(const T (&w)[27]) {
+  T med = w[0];
 #pragma unroll 1
   for (int i = 0; i < 27; ++i) {
     int lt = 0, le = 0;
@@ -59,15 +62,16 @@ __device__ __forceinline__ float median27(const float (&w)[27]) {
 }
 
 // ks^3 median of each component with scipy 'reflect' (== MIRROR fold) at the faces.
-__global__ void median3_kernel(const float* __restrict__ in, int nz, int ny, int nx, int C,
-                               float* __restrict__ out) {
+template <typename T>
+__global__ void median3_kernel(const T* __restrict__ in, int nz, int ny, int nx, int C,
+                               T* __restrict__ out) {
   const int64_t n = (int64_t)nz * ny * nx * C;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
        t += (int64_t)gridDim.x * blockDim.x) {
     const int c = (int)(t % C);
     const int64_t v = t / C;
     const int x = (int)(v % nx), y = (int)((v / nx) % ny), z = (int)(v / ((int64_t)nx * ny));
-    float w[27];
+    T w[27];
     int m = 0;
 #pragma unroll
     for (int a = -1; a <= 1; ++a) {
@@ -87,8 +91,9 @@ __global__ void median3_kernel(const float* __restrict__ in, int nz, int ny, int
 }
 
 // Generic odd window (ks = 5 or 7): partial selection sort in local memory up to the median rank.
-__global__ void median_generic_kernel(const float* __restrict__ in, int nz, int ny, int nx, int C,
-                                      int ks, float* __restrict__ out) {
+template <typename T>
+__global__ void median_generic_kernel(const T* __restrict__ in, int nz, int ny, int nx, int C,
+                                      int ks, T* __restrict__ out) {
   const int64_t n = (int64_t)nz * ny * nx * C;
   const int r = ks / 2, cnt = ks * ks * ks;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
@@ -96,7 +101,7 @@ __global__ void median_generic_kernel(const float* __restrict__ in, int nz, int 
     const int c = (int)(t % C);
     const int64_t v = t / C;
     const int x = (int)(v % nx), y = (int)((v / nx) % ny), z = (int)(v / ((int64_t)nx * ny));
-    float w[343];
+    T w[343];
     int m = 0;
     for (int a = -r; a <= r; ++a)
       for (int b = -r; b <= r; ++b)
@@ -109,7 +114,7 @@ __global__ void median_generic_kernel(const float* __restrict__ in, int nz, int 
       int best = i;
       for (int j = i + 1; j < cnt; ++j)
         if (w[j] < w[best]) best = j;
-      const float tmp = w[i]; w[i] = w[best]; w[best] = tmp;
+      const T tmp = w[i]; w[i] = w[best]; w[best] = tmp;
     }
     out[t] = w[rank];
   }
@@ -125,32 +130,55 @@ unsigned grid_for(int64_t n, int threads) {
 
 using namespace svs;
 
-extern "C" {
+namespace svs {
+namespace {
 
-svs_status svs_gauss_blur3d(const float* in, int nz, int ny, int nx, const float* weights_host,
-                            int r, float* out, svs_stream_t stream) {
-  SVS_REQUIRE(in && out && weights_host, "svs_gauss_blur3d: null pointer");
-  SVS_REQUIRE(nz > 0 && ny > 0 && nx > 0, "svs_gauss_blur3d: bad sizes");
+template <typename T>
+svs_status gauss_blur3d(const char* nm, const T* in, int nz, int ny, int nx, const T* weights_host, int r, T* out,
+                        cudaStream_t stream) {
+  SVS_REQUIRE(in && out && weights_host, std::string(nm) + ": null pointer");
+  SVS_REQUIRE(nz > 0 && ny > 0 && nx > 0, std::string(nm) + ": bad sizes");
   SVS_REQUIRE(r >= 0 && (2 * r + 1) * (2 * r + 1) * (2 * r + 1) <= kMaxBlurTaps,
-              "svs_gauss_blur3d: kernel radius out of range (max 6)");
-  BlurWeights W;
+              std::string(nm) + ": kernel radius out of range (max 6)");
+  BlurWeights<T> W;
   const int k = 2 * r + 1;
   for (int i = 0; i < k * k * k; ++i) W.w[i] = weights_host[i];
   const int64_t n = (int64_t)nz * ny * nx;
-  blur_kernel<<<grid_for(n, 256), 256, 0, stream>>>(in, nz, ny, nx, r, W, out);
-  return check_launch("svs_gauss_blur3d");
+  blur_kernel<T><<<grid_for(n, 256), 256, 0, stream>>>(in, nz, ny, nx, r, W, out);
+  return check_launch(nm);
 }
 
-svs_status svs_median3d(const float* in, int nz, int ny, int nx, int C, int ks, float* out,
-                        svs_stream_t stream) {
-  SVS_REQUIRE(in && out, "svs_median3d: null pointer");
-  SVS_REQUIRE(nz > 0 && ny > 0 && nx > 0 && C > 0, "svs_median3d: bad sizes");
-  SVS_REQUIRE(ks == 1 || ks == 3 || ks == 5 || ks == 7, "svs_median3d: kernel size must be 1, 3, 5 or 7");
+template <typename T>
+svs_status median3d(const char* nm, const T* in, int nz, int ny, int nx, int C, int ks, T* out, cudaStream_t stream) {
+  SVS_REQUIRE(in && out, std::string(nm) + ": null pointer");
+  SVS_REQUIRE(nz > 0 && ny > 0 && nx > 0 && C > 0, std::string(nm) + ": bad sizes");
+  SVS_REQUIRE(ks == 1 || ks == 3 || ks == 5 || ks == 7, std::string(nm) + ": kernel size must be 1, 3, 5 or 7");
   const int64_t n = (int64_t)nz * ny * nx * C;
-  if (ks == 1) return check_cuda(cudaMemcpyAsync(out, in, n * sizeof(float), cudaMemcpyDeviceToDevice, stream), "svs_median3d");
-  if (ks == 3) median3_kernel<<<grid_for(n, 256), 256, 0, stream>>>(in, nz, ny, nx, C, out);
-  else median_generic_kernel<<<grid_for(n, 128), 128, 0, stream>>>(in, nz, ny, nx, C, ks, out);
-  return check_launch("svs_median3d");
+  if (ks == 1) return check_cuda(cudaMemcpyAsync(out, in, n * sizeof(T), cudaMemcpyDeviceToDevice, stream), nm);
+  if (ks == 3) median3_kernel<T><<<grid_for(n, 256), 256, 0, stream>>>(in, nz, ny, nx, C, out);
+  else median_generic_kernel<T><<<grid_for(n, 128), 128, 0, stream>>>(in, nz, ny, nx, C, ks, out);
+  return check_launch(nm);
+}
+
+}  // namespace
+}  // namespace svs
+
+extern "C" {
+
+svs_status svs_gauss_blur3d(const float* in, int nz, int ny, int nx, const float* weights_host, int r, float* out,
+                            svs_stream_t stream) {
+  return gauss_blur3d<float>("svs_gauss_blur3d", in, nz, ny, nx, weights_host, r, out, stream);
+}
+svs_status svs_gauss_blur3d_f64(const double* in, int nz, int ny, int nx, const double* weights_host, int r,
+                                double* out, svs_stream_t stream) {
+  return gauss_blur3d<double>("svs_gauss_blur3d_f64", in, nz, ny, nx, weights_host, r, out, stream);
+}
+svs_status svs_median3d(const float* in, int nz, int ny, int nx, int C, int ks, float* out, svs_stream_t stream) {
+  return median3d<float>("svs_median3d", in, nz, ny, nx, C, ks, out, stream);
+}
+svs_status svs_median3d_f64(const double* in, int nz, int ny, int nx, int C, int ks, double* out,
+                            svs_stream_t stream) {
+  return median3d<double>("svs_median3d_f64", in, nz, ny, nx, C, ks, out, stream);
 }
 
 }  // extern "C"

@@ -59,16 +59,18 @@ def gaussian_kernel3d(sigma: float) -> torch.Tensor:
 
 def apply_gaussian_blur3d(vol: torch.Tensor, sigma: float) -> torch.Tensor:
     """Zero-padded 3D blur with the reference kernel (flow_utils.py:94-112), on the GPU."""
-    if vol.device.type != "cuda" or vol.dtype != torch.float32 or vol.dim() != 3:
-        raise RuntimeError("apply_gaussian_blur3d: expected a 3D float32 CUDA tensor")
+    if vol.device.type != "cuda" or vol.dtype not in (torch.float32, torch.float64) or vol.dim() != 3:
+        raise RuntimeError("apply_gaussian_blur3d: expected a 3D float32 or float64 CUDA tensor")
     vol = vol.contiguous()
-    w = gaussian_kernel3d(sigma).numpy().astype(np.float32)
+    f64 = vol.dtype == torch.float64
+    # the kernel is built in float32 as the reference builds it, then taken to the volume's type
+    w = np.ascontiguousarray(gaussian_kernel3d(sigma).numpy().astype(np.float64 if f64 else np.float32))
     r = w.shape[0] // 2
     out = torch.empty_like(vol)
     nz, ny, nx = vol.shape
+    fn = _lib.lib().svs_gauss_blur3d_f64 if f64 else _lib.lib().svs_gauss_blur3d
     with torch.cuda.device(vol.device):
-        check(_lib.lib().svs_gauss_blur3d(ptr(vol), nz, ny, nx, w.ctypes.data, r, ptr(out),
-                                          stream_ptr(vol.device)))
+        check(fn(ptr(vol), nz, ny, nx, w.ctypes.data, r, ptr(out), stream_ptr(vol.device)))
     return out
 
 
@@ -77,12 +79,14 @@ def apply_median_filter(u: torch.Tensor, ks: int, device: torch.device = None) -
     on the GPU; the result is returned on `device` (default: u's device)."""
     if u.device.type != "cuda":
         raise RuntimeError("apply_median_filter: expected a CUDA tensor")
-    x = u.detach().float().contiguous()
+    x = u.detach()
+    x = (x if x.dtype == torch.float64 else x.float()).contiguous()
     nz, ny, nx = x.shape[:3]
     C = 1 if x.dim() == 3 else int(np.prod(x.shape[3:]))
     out = torch.empty_like(x)
+    fn = _lib.lib().svs_median3d_f64 if x.dtype == torch.float64 else _lib.lib().svs_median3d
     with torch.cuda.device(x.device):
-        check(_lib.lib().svs_median3d(ptr(x), nz, ny, nx, C, int(ks), ptr(out), stream_ptr(x.device)))
+        check(fn(ptr(x), nz, ny, nx, C, int(ks), ptr(out), stream_ptr(x.device)))
     return out if device is None else out.to(device)
 
 

@@ -3,7 +3,8 @@
 
 Same class names, constructor arguments, method names, argument meanings and tensor layouts as the
 reference. Differences a caller can observe:
-  * tensors must be float32 CUDA tensors (the reference also dispatched float64);
+  * tensors must be float32 or float64 CUDA tensors, all of one type within a call (the
+    reference's dispatch took the first tensor's type and reinterpreted the others);
   * kernels run on torch's current CUDA stream (the reference used the legacy default stream);
   * launch errors raise (the reference ignored them, svs/src/cudaDebug.cuh:15-27).
 Argument errors raise RuntimeError, as the reference's TORCH_CHECK / CHECK_INPUT did.
@@ -71,16 +72,22 @@ class MeshInfo3D:
 
 
 # ------------------------------------------------------------------------------- helpers
+def _op(name: str, t: torch.Tensor):
+    """The entry point for the tensor's value type: float32 -> name, float64 -> name_f64 (the
+    reference dispatched both, AT_DISPATCH_FLOATING_TYPES)."""
+    return getattr(_lib.lib(), name + ("_f64" if t.dtype == torch.float64 else ""))
+
+
 def _check_input(t: torch.Tensor, name: str) -> None:
-    """CHECK_INPUT of coreDefines.h:10-12, plus the float32 requirement of this library."""
+    """CHECK_INPUT of coreDefines.h:10-12, plus the float32 / float64 requirement."""
     if not isinstance(t, torch.Tensor):
         raise TypeError(f"{name} must be a torch.Tensor")
     if t.device.type != "cuda":
         raise RuntimeError(f"{name} must be a CUDA tensor")
     if not t.is_contiguous():
         raise RuntimeError(f"{name} must be contiguous")
-    if t.dtype != torch.float32:
-        raise RuntimeError(f"{name} must be float32 (got {t.dtype})")
+    if t.dtype not in (torch.float32, torch.float64):
+        raise RuntimeError(f"{name} must be float32 or float64 (got {t.dtype})")
 
 
 def _check_dim(t: torch.Tensor, d: int) -> None:
@@ -93,6 +100,8 @@ def _same_device(*ts):
     for t in ts[1:]:
         if t.device != dev:
             raise RuntimeError("all tensors must be on the same CUDA device")
+        if t.dtype != ts[0].dtype:
+            raise RuntimeError("all tensors must have the same dtype")
     return dev
 
 
@@ -109,7 +118,7 @@ class Nabla3D_CD:
         out = torch.empty(tuple(b.shape) + (3,), dtype=b.dtype, device=b.device)
         hz, hy, hx = self._mesh.h()
         with torch.cuda.device(b.device):
-            check(_lib.lib().svs_nabla3d_forward(ptr(b), nz, ny, nx, C, hz, hy, hx, self._bdry,
+            check(_op("svs_nabla3d_forward", b)(ptr(b), nz, ny, nx, C, hz, hy, hx, self._bdry,
                                                  ptr(out), stream_ptr(b.device)))
         return out
 
@@ -118,7 +127,7 @@ class Nabla3D_CD:
         out = torch.empty(tuple(p.shape[:-1]), dtype=p.dtype, device=p.device)
         hz, hy, hx = self._mesh.h()
         with torch.cuda.device(p.device):
-            check(_lib.lib().svs_nabla3d_backward(ptr(p), nz, ny, nx, C, hz, hy, hx, self._bdry,
+            check(_op("svs_nabla3d_backward", p)(ptr(p), nz, ny, nx, C, hz, hy, hx, self._bdry,
                                                   ptr(out), stream_ptr(p.device)))
         return out
 
@@ -164,7 +173,7 @@ class AnisotropicNabla3D:
         s = torch.empty(sh, dtype=g.dtype, device=g.device)
         n, t1, t2 = (torch.empty(sh + (3,), dtype=g.dtype, device=g.device) for _ in range(3))
         with torch.cuda.device(g.device):
-            check(_lib.lib().svs_aniso3d_tangents(ptr(g), int(np.prod(sh)), self._alpha, self._beta,
+            check(_op("svs_aniso3d_tangents", g)(ptr(g), int(np.prod(sh)), self._alpha, self._beta,
                                                   ptr(s), ptr(n), ptr(t1), ptr(t2), stream_ptr(g.device)))
         return [s, n, t1, t2]
 
@@ -179,7 +188,7 @@ class AnisotropicNabla3D:
         _same_device(b, scalars, normals, tangents1, tangents2)
         out = torch.empty_like(b)
         with torch.cuda.device(b.device):
-            check(_lib.lib().svs_aniso3d_apply(ptr(b), nvox, ptr(scalars), ptr(normals), ptr(tangents1),
+            check(_op("svs_aniso3d_apply", b)(ptr(b), nvox, ptr(scalars), ptr(normals), ptr(tangents1),
                                                ptr(tangents2), ptr(out), stream_ptr(b.device)))
         return out
 
@@ -205,7 +214,7 @@ class Warping3D:
         out = torch.empty_like(u)
         hz, hy, hx = self._mesh.h()
         with torch.cuda.device(u.device):
-            check(_lib.lib().svs_warp3d(ptr(u), nz, ny, nx, C, ptr(phi), hz, hy, hx, self._interp,
+            check(_op("svs_warp3d", u)(ptr(u), nz, ny, nx, C, ptr(phi), hz, hy, hx, self._interp,
                                         self._bdry, ptr(out), stream_ptr(u.device)))
         return out
 
@@ -237,7 +246,7 @@ class Warping3D:
         gp = torch.empty_like(phi)
         hz, hy, hx = self._mesh.h()
         with torch.cuda.device(u.device):
-            check(_lib.lib().svs_warp3d_backward(ptr(u), nz, ny, nx, ptr(phi), ptr(forward_out), hz, hy,
+            check(_op("svs_warp3d_backward", u)(ptr(u), nz, ny, nx, ptr(phi), ptr(forward_out), hz, hy,
                                                  hx, self._interp, self._bdry, ptr(gu), ptr(gp),
                                                  stream_ptr(u.device)))
         return [gu, gp]
@@ -263,7 +272,7 @@ class WarpingCNN3D:
         out = torch.empty_like(u)
         hz, hy, hx = self._mesh.h()
         with torch.cuda.device(u.device):
-            check(_lib.lib().svs_warp_cnn3d(ptr(u), B, C, nz, ny, nx, ptr(phi), hz, hy, hx, self._interp,
+            check(_op("svs_warp_cnn3d", u)(ptr(u), B, C, nz, ny, nx, ptr(phi), hz, hy, hx, self._interp,
                                             self._bdry, ptr(out), stream_ptr(u.device)))
         return out
 
@@ -287,7 +296,7 @@ class Prolongation3D:
         out = torch.empty((tz, ty, tx) + tuple(tail), dtype=u.dtype, device=u.device)
         s = self._src
         with torch.cuda.device(u.device):
-            check(_lib.lib().svs_prolongate3d(ptr(u), nz, ny, nx, C, s.getLZ(), s.getLY(), s.getLX(),
+            check(_op("svs_prolongate3d", u)(ptr(u), nz, ny, nx, C, s.getLZ(), s.getLY(), s.getLX(),
                                               tz, ty, tx, d.getLZ(), d.getLY(), d.getLX(), self._interp,
                                               self._bdry, ptr(out), stream_ptr(u.device)))
         return out
@@ -328,7 +337,7 @@ def TVL1OF3D_proxPrimal(primalVariable: torch.Tensor, primalStepSize_tau: float,
     out = torch.empty_like(primalVariable)
     dev = primalVariable.device
     with torch.cuda.device(dev):
-        check(_lib.lib().svs_tvl1_prox_primal(ptr(primalVariable), n, float(primalStepSize_tau),
+        check(_op("svs_tvl1_prox_primal", primalVariable)(ptr(primalVariable), n, float(primalStepSize_tau),
                                               float(primalFctWeight_Matching), ptr(rho), ptr(I1_warped_grad),
                                               ptr(out), stream_ptr(dev)))
     return out
@@ -346,7 +355,7 @@ def TVL1OF3D_proxDual(dualVariable: torch.Tensor, dualStepSize_sigma: float, dua
     out = torch.empty_like(dualVariable)
     dev = dualVariable.device
     with torch.cuda.device(dev):
-        check(_lib.lib().svs_tvl1_prox_dual(ptr(dualVariable), n, float(dualStepSize_sigma),
+        check(_op("svs_tvl1_prox_dual", dualVariable)(ptr(dualVariable), n, float(dualStepSize_sigma),
                                             float(dualFctWeight_TV), ptr(out), stream_ptr(dev)))
     return out
 

@@ -252,12 +252,14 @@ class TVL13DOpticalFlow:
             I0s.append(op.forward(I0s[s - 1]))
             I1s.append(op.forward(I1s[s - 1]))
             m = mesh_infos[s]
-            us.append(torch.zeros([m.getNZ(), m.getNY(), m.getNX(), 3], dtype=torch.float32, device=self.device))
-            ps.append(torch.zeros([m.getNZ(), m.getNY(), m.getNX(), 3, 3], dtype=torch.float32, device=self.device))
+            us.append(torch.zeros([m.getNZ(), m.getNY(), m.getNX(), 3], dtype=I0.dtype, device=self.device))
+            ps.append(torch.zeros([m.getNZ(), m.getNY(), m.getNX(), 3, 3], dtype=I0.dtype, device=self.device))
         return I0s, I1s, us, ps, mesh_infos
 
     def compute_unfused(self, I0, I1, u, p):
-        """tvl13d.py:122-162 exactly as the reference structures it (per-operator launches)."""
+        """tvl13d.py:122-162 exactly as the reference structures it (per-operator launches), in
+        the inputs' type: float32 (the plain GPU form) or float64 (an FP64 GPU run of the same
+        algorithm, the fast oracle for large volumes)."""
         I0s, I1s, us, ps, mesh_infos = self.generate_pyramid(I0, I1, u, p)
         for s in range(self.num_scales - 1, -1, -1):
             us[s], ps[s] = self.step(s, I0s[s], I1s[s], us[s], ps[s], mesh_infos[s])
@@ -279,8 +281,8 @@ class TVL13DOpticalFlow:
         warping_op = opticalFlow.Warping3D(meshInfo, self.interpolation_type, self.boundary_type)
         I1_grad = nabla_op.forward(I1)
         shape = (meshInfo.getNZ(), meshInfo.getNY(), meshInfo.getNX())
-        scalars = torch.zeros(shape, dtype=torch.float32, device=self.device)
-        normals = torch.zeros(shape + (3,), dtype=torch.float32, device=self.device)
+        scalars = torch.zeros(shape, dtype=I1.dtype, device=self.device)
+        normals = torch.zeros(shape + (3,), dtype=I1.dtype, device=self.device)
         tangents1 = torch.zeros_like(normals)
         tangents2 = torch.zeros_like(normals)
         if self.use_anisotropic_diff:
