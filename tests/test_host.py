@@ -131,3 +131,12 @@ def test_poisson_stream_shape():
     assert 5 <= len(reqs) <= 40
     for t, T, dims in reqs:
         assert 12 <= T <= 35 and all(64 <= d <= 128 and d % 8 == 0 for d in dims)
+
+
+def test_time_pading_zero_pads_the_time_axis():
+    import torch
+    from singleventriclesegmentation_b200.preprocessing import time_pading
+    x = torch.arange(2 * 3 * 4 * 5, dtype=torch.float32).reshape(2, 3, 4, 5)
+    y = time_pading(8, x)
+    assert y.shape == (2, 3, 4, 8)
+    assert torch.equal(y[..., :5], x) and torch.count_nonzero(y[..., 5:]) == 0
