@@ -25,7 +25,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -495,9 +494,8 @@ def main():
     d_masks = host_masks.to(dev)
     flows = torch.empty((n_pairs,) + SHAPE + (3,), dtype=torch.float32, device=dev)
     plan = solver.plan_for([SHAPE] * n_pairs)
-    level_tiles_tuned = None
     if not args.no_autotune:
-        level_tiles_tuned = tune_plan(plan, args.storage)
+        tune_plan(plan, args.storage)
     fwd_idx = list(range(MASK_T0, MASK_T1))                       # forward pairs t -> t+1
     bwd_idx = [(T - 1) + (T - 1 - t) for t in range(MASK_T1, MASK_T0, -1)]  # backward pairs t -> t-1
 

@@ -6,7 +6,7 @@ used cuDNN conv3d and a host round trip through scipy).
 """
 from __future__ import annotations
 
-from typing import Literal, Tuple, Union
+from typing import Tuple
 
 import numpy as np
 import torch

@@ -10,7 +10,7 @@ one batch; the median filter runs on the device inside the solve.
 from __future__ import annotations
 
 import os
-from typing import List, Sequence, Tuple
+from typing import List, Tuple
 
 import numpy as np
 import torch

@@ -22,7 +22,6 @@ from __future__ import annotations
 
 import collections
 import concurrent.futures as cf
-import math
 import threading
 import time
 from dataclasses import dataclass, field

@@ -12,7 +12,7 @@ from __future__ import annotations
 import collections
 import ctypes
 import math
-from typing import List, Literal, Optional, Sequence, Tuple
+from typing import Literal, Optional, Sequence, Tuple
 
 import numpy as np
 import torch

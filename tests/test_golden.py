@@ -98,7 +98,6 @@ def test_oracle_masks_match_reference(oracle):
 @pytest.mark.gpu
 def test_kernels_match_reference_operators(cuda):
     from singleventriclesegmentation_b200 import opticalFlow as of
-    from singleventriclesegmentation_b200.flow_utils import apply_median_filter  # noqa: F401
     d = load("ref_ops.npz")
     T = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device="cuda")
     N = lambda t: t.cpu().numpy()

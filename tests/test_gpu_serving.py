@@ -5,7 +5,7 @@ import pytest
 import torch
 
 from singleventriclesegmentation_b200 import synthetic
-from singleventriclesegmentation_b200.serving import FlowServer, poisson_requests
+from singleventriclesegmentation_b200.serving import FlowServer
 
 pytestmark = [pytest.mark.gpu, pytest.mark.timeout(600)]
 
