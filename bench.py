@@ -16,6 +16,7 @@ metric asks for. Further workloads, one JSON line each, on one GPU:
     python bench.py --workload uneven    # 64 pairs, dims per axis on {40, ..., 128}
     python bench.py --workload mixed     # the sequence + 16 x 128^3, 16-bit storage modes, EPE vs FP64 GPU oracle
     python bench.py --workload serving   # Poisson request streams through the continuous-batching server
+    python bench.py --workload latency   # p50/p99 of one 80^3 pair alone and of the 68-pair sequence
 
 Multi-GPU: one process per GPU (torchrun); every rank solves its own sequence (replicas, weak
 scaling, no collective on the data path); NCCL is used only for the barrier and the max-over-ranks
@@ -55,11 +56,12 @@ def parse():
     ap.add_argument("--no-plain-form", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--frames", type=int, default=T_FRAMES)
-    ap.add_argument("--workload", default="sequence", choices=["sequence", "uneven", "mixed", "serving"],
+    ap.add_argument("--workload", default="sequence", choices=["sequence", "uneven", "mixed", "serving", "latency"],
                     help="sequence: 35-frame 80^3 cine sequence (the headline line); uneven: 64 pairs of "
                          "mixed sizes; mixed: the sequence plus 16 pairs of 128^3 with EPE against the FP64 "
                          "oracle; serving: Poisson request stream through the continuous-batching server")
     ap.add_argument("--rates", default="0.1,1,10,50", help="serving: arrival rates (requests/s)")
+    ap.add_argument("--reps", type=int, default=50, help="latency: repetitions of the single-pair solve")
     ap.add_argument("--requests", type=int, default=6, help="serving: requests per rate")
     ap.add_argument("--max-active", type=int, default=2, help="serving: requests on the device at once")
     return ap.parse_args()
@@ -452,6 +454,59 @@ def run_serving(args):
                       "results": results}), flush=True)
 
 
+def run_latency(args):
+    """Latency: one 80^3 pair (the blob / sine-displacement pair, default configuration) solved
+    alone through TVL13DOpticalFlow.compute, --reps times, and the 68-pair sequence solve plus mask
+    propagation, max(5, reps // 5) times; each repetition timed with CUDA events around the call
+    and a synchronisation; p50/p99/mean in seconds."""
+    import torch
+    from singleventriclesegmentation_b200 import synthetic
+    from singleventriclesegmentation_b200.warping import Warp, propagate_batched
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    st = torch.cuda.current_stream(dev)
+
+    def timed(fn, reps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize(dev)
+        out = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            fn()
+            e1.record(st)
+            torch.cuda.synchronize(dev)
+            out.append(e0.elapsed_time(e1) / 1000.0)
+        a = np.array(out)
+        return {"p50_s": float(np.percentile(a, 50)), "p99_s": float(np.percentile(a, 99)),
+                "mean_s": float(a.mean()), "reps": reps}
+
+    I0, I1, _ = synthetic.frame_pair(SHAPE, seed=0, device="cuda")
+    I0, I1 = torch.from_numpy(I0).to(dev), torch.from_numpy(I1).to(dev)
+    solver = _solver(dev, args.storage)
+    pair = timed(lambda: solver.compute(I0, I1), args.reps, 3)
+
+    T = T_FRAMES
+    seq = torch.from_numpy(synthetic.cine_sequence(T=T, shape=SHAPE, seed=0, device="cuda")).to(dev)
+    pairs = synthetic.sequence_pairs(T, "forward") + synthetic.sequence_pairs(T, "backward")
+    masks = torch.from_numpy(np.stack([synthetic.ellipsoid_mask(SHAPE, (15, 12, 10)),
+                                       synthetic.ellipsoid_mask(SHAPE, (13, 12, 10))])[:, None]).to(dev)
+    flows = torch.empty((len(pairs),) + SHAPE + (3,), device=dev)
+    plan = solver.plan_for([SHAPE] * len(pairs))
+    warp = Warp("CUBIC_HERMITESPLINE", "MIRROR", "numDofs", (1, 1, 1))
+    fwd_idx = list(range(MASK_T0, MASK_T1))
+    bwd_idx = [(T - 1) + (T - 1 - t) for t in range(MASK_T1, MASK_T0, -1)]
+
+    def sequence():
+        plan.solve([seq[a] for a, b in pairs], [seq[b] for a, b in pairs], [flows[i] for i in range(len(pairs))])
+        propagate_batched(warp, masks, torch.stack([flows[fwd_idx], flows[bwd_idx]], dim=1))
+
+    seq_lat = timed(sequence, max(5, args.reps // 5), 2)
+    print(json.dumps({"metric": "latency p50/p99", "unit": "s", "storage": args.storage, "data": "synthetic",
+                      "pair_80cube": pair, "sequence_35x80cube_68pairs_with_masks": seq_lat}), flush=True)
+
+
 # ------------------------------------------------------------------------------ our arm
 def main():
     args = parse()
@@ -459,7 +514,7 @@ def main():
         reference_arm(args)
         return
     if args.workload != "sequence":
-        {"uneven": run_uneven, "mixed": run_mixed, "serving": run_serving}[args.workload](args)
+        {"uneven": run_uneven, "mixed": run_mixed, "serving": run_serving, "latency": run_latency}[args.workload](args)
         return
     import torch
     import torch.distributed as dist
