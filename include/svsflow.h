@@ -229,6 +229,10 @@ svs_status svs_tvl1_plan_set_level_tile(svs_plan* plan, int level, int tile_id);
  * variant than the level's form a group per variant; the groups run concurrently (parallel
  * branches of the solve's graph). Used by the autotuner to pick variants per size class. */
 svs_status svs_tvl1_plan_set_pair_tile(svs_plan* plan, int level, int pair, int tile_id);
+/* Number of z chunks each column tile of a level is split into (0 = the automatic choice: the
+ * wave model for the TMA-pipeline variants). More chunks mean more CTAs, each marching fewer
+ * planes. Used by the autotuner. */
+svs_status svs_tvl1_plan_set_level_chunks(svs_plan* plan, int level, int chunks);
 int svs_tvl1_num_tiles(void);
 
 /* Residuals. With record != 0 every later solve logs, after each warp of each level, the

@@ -84,6 +84,7 @@ _SIGS = {
     "svs_tvl1_plan_set_level_tile": (c_int, [c_void_p, c_int, c_int]),
     "svs_tvl1_num_tiles": (c_int, []),
     "svs_tvl1_plan_set_pair_tile": (c_int, [c_void_p, c_int, c_int, c_int]),
+    "svs_tvl1_plan_set_level_chunks": (c_int, [c_void_p, c_int, c_int]),
     "svs_tvl1_plan_set_residuals": (c_int, [c_void_p, c_int, c_float]),
     "svs_tvl1_plan_get_residuals": (c_int, [c_void_p, c_void_p, c_size_t]),
     "svs_tvl1_tile_info": (c_int, [c_int, ctypes.POINTER(c_int), ctypes.POINTER(c_int), ctypes.POINTER(c_int),

@@ -187,6 +187,7 @@ def _main(argv=None) -> None:
     ap.add_argument("--tiles", default="")
     ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--level", type=int, default=0)
+    ap.add_argument("--chunks", default="0", help="z chunks per column to try at the level (0 = automatic)")
     args = ap.parse_args(argv)
     dev = torch.device("cuda", 0)
     shape = (args.size,) * 3
@@ -204,11 +205,16 @@ def _main(argv=None) -> None:
             plan.solve([I0] * args.pairs, [I1] * args.pairs, outs)
             torch.cuda.synchronize()
             plan.check()
-            ms = time_variant(plan, args.level, tid, args.iters)
-            plan.check()
             vox = args.pairs * int(np.prod([(n + (1 << args.level) - 1) >> args.level for n in shape]))
-            print(_json.dumps({"storage": args.storage, "tile": tid, "level": args.level, "ms": round(ms, 4),
-                               "GBs": round(vox * bpv / (ms / 1e3) / 1e9, 1)}), flush=True)
+            for ch in [int(c) for c in args.chunks.split(",")]:
+                plan.set_level_chunks(args.level, ch)
+                ms = time_variant(plan, args.level, tid, args.iters)
+                plan.check()
+                line = {"storage": args.storage, "tile": tid, "level": args.level, "ms": round(ms, 4),
+                        "GBs": round(vox * bpv / (ms / 1e3) / 1e9, 1)}
+                if ch:
+                    line["chunks"] = ch
+                print(_json.dumps(line), flush=True)
             plan.close()
         except _lib.SVSError as e:
             print(_json.dumps({"storage": args.storage, "tile": tid, "error": str(e)[:160]}), flush=True)

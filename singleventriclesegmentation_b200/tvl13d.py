@@ -76,6 +76,10 @@ class SolverPlan:
     def level_tiles(self):
         return [int(_lib.lib().svs_tvl1_plan_level_tile(self._h, l)) for l in range(8)]
 
+    def set_level_chunks(self, level: int, chunks: int) -> None:
+        """z chunks per column tile at a level (0 = automatic)."""
+        check(_lib.lib().svs_tvl1_plan_set_level_chunks(self._h, int(level), int(chunks)))
+
     def set_pair_tile(self, level: int, pair: int, tile_id: int) -> None:
         check(_lib.lib().svs_tvl1_plan_set_pair_tile(self._h, int(level), int(pair), int(tile_id)))
 

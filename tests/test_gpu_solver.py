@@ -184,6 +184,33 @@ def test_pair_variant_groups_run_concurrently_with_the_same_result(cuda):
     plan.check()
 
 
+@pytest.mark.parametrize("storage", ["f32", "f16-flow32"])
+def test_z_chunk_overrides_keep_the_result(cuda, storage):
+    """Splitting the columns of a level into more z chunks (svs_tvl1_plan_set_level_chunks, down to
+    one plane per chunk) changes only which CTA computes a plane, not its arithmetic: the result
+    is bitwise that of the automatic split, for the split-role and the plain-load forms."""
+    from singleventriclesegmentation_b200 import _lib
+    shapes = [(21, 37, 45), (24, 24, 24)]
+    pairs = [synthetic.frame_pair(sh, seed=30 + i) for i, sh in enumerate(shapes)]
+    for tid in (0, 6):   # automatic (split-role) and plain-load 32x8
+        solver, _ = make_solver(storage=storage, max_warps=2, max_outer_iterations=20)
+        solver.tile_id = tid
+        ref = solver.compute_batch([T(p[0]) for p in pairs], [T(p[1]) for p in pairs])
+        for chunks in ((1, 1), (3, 7), (24, 12)):
+            solver._plans.clear()
+            plan = solver.plan_for(shapes)
+            for level, c in enumerate(chunks):
+                plan.set_level_chunks(level, c)
+            outs = [torch.empty(sh + (3,), device="cuda") for sh in shapes]
+            plan.solve([T(p[0]) for p in pairs], [T(p[1]) for p in pairs], outs)
+            torch.cuda.synchronize()
+            plan.check()
+            for a, b in zip(ref, outs):
+                assert torch.equal(a, b), (tid, chunks)
+    with pytest.raises(_lib.SVSError):
+        plan.set_level_chunks(5, 2)
+
+
 def test_graph_reuse_and_new_inputs(cuda):
     solver, _ = make_solver(max_warps=2, max_outer_iterations=20)
     a = synthetic.frame_pair((16, 16, 16), seed=1)
