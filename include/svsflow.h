@@ -266,6 +266,9 @@ svs_status svs_tvl1_bench_iterations(svs_plan* plan, int level, int count, svs_s
 uint64_t svs_tvl1_plan_graph_kernels(const svs_plan* plan);
 /* Iterate-kernel variant the plan uses at a pyramid level (after the first solve; 0 before). */
 int svs_tvl1_plan_level_tile(const svs_plan* plan, int level);
+/* CTAs of one iteration at a pyramid level, all variant groups together (after the first solve;
+ * 0 before): the column tiles times their z chunks. */
+int64_t svs_tvl1_plan_level_ctas(const svs_plan* plan, int level);
 /* Synchronous check of the plan's device status: SVS_ERR_TIMEOUT if a bounded pipeline wait
  * inside an iterate kernel gave up (the kernel then returned early and the results of that
  * solve are invalid), SVS_OK otherwise. */

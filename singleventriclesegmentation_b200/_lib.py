@@ -93,6 +93,7 @@ _SIGS = {
     "svs_tvl1_bench_iterations": (c_int, [c_void_p, c_int, c_int, c_void_p]),
     "svs_tvl1_plan_graph_kernels": (ctypes.c_uint64, [c_void_p]),
     "svs_tvl1_plan_level_tile": (c_int, [c_void_p, c_int]),
+    "svs_tvl1_plan_level_ctas": (c_int64, [c_void_p, c_int]),
     "svs_tvl1_plan_check": (c_int, [c_void_p]),
     "svs_tvl1_solve_noalloc": (c_int, [ctypes.POINTER(TVL1Params), c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
 }

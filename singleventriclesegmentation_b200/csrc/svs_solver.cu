@@ -662,34 +662,48 @@ int auto_tile(const svs_plan& P, int level) {
   return widest <= 32 ? kAuto16Narrow : kAuto16;
 }
 
-// z chunks per column for a split-role variant: the count that minimises the launch's makespan
-// in plane steps, waves x (planes per chunk + kFillPlanes), where a wave is one CTA on every
-// resident slot (SMs x CTAs per SM from the occupancy calculator) and kFillPlanes stands for the
-// pipeline start of a chunk (the first DIST planes and the extra dual plane below z0). Chunks go
-// down to one plane: a single 80^3 pair runs a level-1 iteration (40^3, five 40x8 column tiles)
-// 1.7x faster as 200 one-plane chunks than as 25 eight-plane chunks.
+// z chunks per column for a split-role variant. The launch's CTAs are dispatched in tile-list
+// order onto the resident slots (SMs x CTAs per SM from the occupancy calculator). Columns fill
+// whole waves of `main_c` chunks each; the `tail_cols` columns that would leave the last wave
+// part-empty come after them, cut into `tail_c` chunks, so the tail spreads over all slots. The
+// plan minimises the makespan in plane steps, sum over the two phases of waves x (planes per chunk
+// + kFillPlanes), where kFillPlanes stands for the pipeline start of a chunk (the first DIST
+// planes and the extra dual plane below z0). Chunks go down to one plane: a single 80^3 pair runs
+// a level-1 iteration (40^3, five 40x8 column tiles) 1.7x faster as 200 one-plane chunks than as
+// 25 eight-plane chunks.
 constexpr int kFillPlanes = 3;
-int split_chunks(const svs_plan& P, int level, int tid, long long xy_tiles) {
+struct ChunkPlan {
+  int main_c = 1, tail_c = 1;
+  long long tail_cols = 0;  // the last tail_cols columns of the tile list use tail_c
+};
+ChunkPlan split_chunks(const svs_plan& P, int level, int tid, long long xy_tiles) {
+  ChunkPlan best;
   int dev = 0, sms = 148, per_sm = 0, nz = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int box[4] = {0, 0, 0, 0};
   const TileShape& ts = kTileShapes[tid - 1];
   if (!split_variant(P.prm.storage, ts.split, 2, P.prm.boundary != SVS_BOUNDARY_MIRROR, 0, nullptr, nullptr,
-                     nullptr, nullptr, nullptr, nullptr, box))
-    return 1;
+                     nullptr, nullptr, nullptr, nullptr, box) ||
+      xy_tiles <= 0)
+    return best;
   per_sm = std::max(1, box[0]);
   for (int i = 0; i < P.num_pairs; ++i)
     if (!P.pair_mask || (*P.pair_mask)[i]) nz = std::max(nz, P.h_descs[(size_t)level * P.num_pairs + i].nz);
   const long long slots = (long long)sms * per_sm;
-  int best = 1;
   long long best_cost = -1;
-  for (int c = 1; c <= nz; ++c) {
-    const long long waves = (xy_tiles * c + slots - 1) / slots;
-    const long long cost = waves * (ceil_div(nz, c) + kFillPlanes);
-    if (best_cost < 0 || cost < best_cost) {
-      best_cost = cost;
-      best = c;
+  for (int cm = 1; cm <= nz; ++cm) {
+    // columns whose chunks fill whole waves; the rest form the tail
+    const long long main_cols = std::min(xy_tiles, (xy_tiles * cm / slots) * slots / cm);
+    const long long t_main = ceil_div(main_cols * cm, slots) * (ceil_div(nz, cm) + kFillPlanes);
+    const long long rest = xy_tiles - main_cols;
+    for (int ct = cm; ct <= nz; ++ct) {
+      const long long t_tail = rest ? ceil_div(rest * ct, slots) * (ceil_div(nz, ct) + kFillPlanes) : 0;
+      if (best_cost < 0 || t_main + t_tail < best_cost) {
+        best_cost = t_main + t_tail;
+        best = ChunkPlan{cm, rest ? ct : cm, rest};
+      }
+      if (!rest) break;
     }
   }
   return best;
@@ -708,29 +722,44 @@ void build_tiles(svs_plan& P, int level, int tid, std::vector<Tile>* out_opt = n
     const Desc& d = P.h_descs[(size_t)level * P.num_pairs + i];
     xy_tiles += (long long)ceil_div(d.nx, ts.tx) * ceil_div(d.ny, ts.ty);
   }
-  // split-role variants: chunk count from the wave model above; other forms: z is split into
-  // chunks only when the level has too few column tiles to fill the GPU
-  const int split_c = ts.form == kSplit ? split_chunks(P, level, tid, xy_tiles) : 0;
-  const long long target = 148LL * 2;
+  // split-role variants: chunks from the wave model above (the tail columns after the others);
+  // other forms: z is split into chunks only when the level has too few column tiles to fill the
+  // GPU; a per-level request overrides both with one count for every column
+  const int req_c = level < (int)P.level_chunks_req.size() ? P.level_chunks_req[level] : 0;
+  ChunkPlan cp;
+  if (req_c > 0) {
+    cp.main_c = req_c;
+  } else if (ts.form == kSplit) {
+    cp = split_chunks(P, level, tid, xy_tiles);
+  } else {
+    const long long target = 148LL * 2;
+    if (xy_tiles < target) cp.main_c = (int)((target + xy_tiles - 1) / xy_tiles);
+  }
+  const bool plain_cap = req_c <= 0 && ts.form != kSplit;  // at least 8 planes per chunk
+  std::vector<Tile> tail;
+  long long col = 0;
   for (int i = 0; i < P.num_pairs; ++i) {
     if (!in(i)) continue;
     const Desc& d = P.h_descs[(size_t)level * P.num_pairs + i];
-    int chunks = 1;
-    const int req_c = level < (int)P.level_chunks_req.size() ? P.level_chunks_req[level] : 0;
-    if (req_c > 0)
-      chunks = std::min(req_c, d.nz);
-    else if (split_c > 0)
-      chunks = std::min(split_c, d.nz);
-    else if (xy_tiles < target)
-      chunks = (int)std::min<long long>((target + xy_tiles - 1) / xy_tiles, std::max(1, d.nz / 8));
-    const int zc = (d.nz + chunks - 1) / chunks;
-    for (int z0 = 0; z0 < d.nz; z0 += zc)
-      for (int y0 = 0; y0 < d.ny; y0 += ts.ty)
-        for (int x0 = 0; x0 < d.nx; x0 += ts.tx) {
-          const int z1 = std::min(d.nz, z0 + zc);
-          out.push_back(Tile{level * P.num_pairs + i, x0, y0, z0 | (z1 << 16)});
-        }
+    const long long ncols = (long long)ceil_div(d.nx, ts.tx) * ceil_div(d.ny, ts.ty);
+    // within a pair, chunk by chunk (the columns of one z range next to each other)
+    for (int part = 0; part < 2; ++part) {
+      int chunks = part ? cp.tail_c : cp.main_c;
+      chunks = std::max(1, std::min(chunks, plain_cap ? std::max(1, d.nz / 8) : d.nz));
+      const int zc = (d.nz + chunks - 1) / chunks;
+      for (int z0 = 0; z0 < d.nz; z0 += zc) {
+        long long c = col;
+        for (int y0 = 0; y0 < d.ny; y0 += ts.ty)
+          for (int x0 = 0; x0 < d.nx; x0 += ts.tx, ++c) {
+            if ((c >= xy_tiles - cp.tail_cols) != (part == 1)) continue;
+            const int z1 = std::min(d.nz, z0 + zc);
+            (part ? tail : out).push_back(Tile{level * P.num_pairs + i, x0, y0, z0 | (z1 << 16)});
+          }
+      }
+    }
+    col += ncols;
   }
+  out.insert(out.end(), tail.begin(), tail.end());
 }
 
 // (Re)build tile lists and TMA descriptors for the requested tile id.
@@ -1309,6 +1338,14 @@ uint64_t svs_tvl1_plan_graph_kernels(const svs_plan* P) { return P ? P->graph_ke
 
 int svs_tvl1_plan_level_tile(const svs_plan* P, int level) {
   return (P && level >= 0 && level < (int)P->level_tile.size()) ? P->level_tile[level] : 0;
+}
+
+int64_t svs_tvl1_plan_level_ctas(const svs_plan* P, int level) {
+  if (!P || level < 0 || level >= (int)P->h_tiles.size()) return 0;
+  int64_t n = (int64_t)P->h_tiles[level].size();
+  if (level < (int)P->extra.size())
+    for (const auto& grp : P->extra[level]) n += (int64_t)grp.h.size();
+  return n;
 }
 
 svs_status svs_tvl1_plan_check(svs_plan* P) {

@@ -76,6 +76,10 @@ class SolverPlan:
     def level_tiles(self):
         return [int(_lib.lib().svs_tvl1_plan_level_tile(self._h, l)) for l in range(8)]
 
+    def level_ctas(self, level: int) -> int:
+        """CTAs of one iterate launch at `level` (all variant groups; 0 before the first solve)."""
+        return int(_lib.lib().svs_tvl1_plan_level_ctas(self._h, int(level)))
+
     def set_level_chunks(self, level: int, chunks: int) -> None:
         """z chunks per column tile at a level (0 = automatic)."""
         check(_lib.lib().svs_tvl1_plan_set_level_chunks(self._h, int(level), int(chunks)))

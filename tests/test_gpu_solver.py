@@ -211,6 +211,41 @@ def test_z_chunk_overrides_keep_the_result(cuda, storage):
         plan.set_level_chunks(5, 2)
 
 
+def test_tail_columns_split_into_chunks_keep_the_result(cuda):
+    """A batch whose column tiles overfill the resident CTA slots: the columns beyond the last
+    full wave are cut into z chunks placed at the end of the launch, the other columns march whole.
+    Every pair's result is bitwise that of one chunk per column."""
+    # 34 pairs of 48^3 in 16x16 column tiles: 306 columns, which for 1 to 6 resident CTAs per SM
+    # leave both whole-wave columns and a split tail
+    shape = (48, 48, 48)
+    n = 34
+    pairs = [synthetic.frame_pair(shape, seed=40 + i % 4) for i in range(n)]
+    solver, _ = make_solver(storage="f16-flow32", num_scales=1, max_warps=1, max_outer_iterations=10)
+    plan = solver.plan_for([shape] * n)
+    outs = [torch.empty(shape + (3,), device="cuda") for _ in range(n)]
+    plan.solve([T(p[0]) for p in pairs], [T(p[1]) for p in pairs], outs)
+    torch.cuda.synchronize()
+    plan.check()
+    tid = plan.level_tiles()[0]
+    info = _lib_tile_info(tid)
+    cols = n * -(-shape[1] // info["ty"]) * -(-shape[2] // info["tx"])
+    auto_ctas = plan.level_ctas(0)
+    assert auto_ctas > cols   # the tail columns were split
+    plan.set_level_chunks(0, 1)
+    ref = [torch.empty_like(o) for o in outs]
+    plan.solve([T(p[0]) for p in pairs], [T(p[1]) for p in pairs], ref)
+    torch.cuda.synchronize()
+    plan.check()
+    assert plan.level_ctas(0) == cols
+    for a, b in zip(ref, outs):
+        assert torch.equal(a, b)
+
+
+def _lib_tile_info(tid):
+    from singleventriclesegmentation_b200 import _lib
+    return _lib.tile_info(tid)
+
+
 def test_graph_reuse_and_new_inputs(cuda):
     solver, _ = make_solver(max_warps=2, max_outer_iterations=20)
     a = synthetic.frame_pair((16, 16, 16), seed=1)
