@@ -127,17 +127,26 @@ __device__ __forceinline__ float2 shrink_step(float2 rho, float2 g2s, float fact
 
 // Primal update, tvl13d.py:229-235 with opticalFlowOps.cu:123-175: rho = rc + u.g (u before
 // the update), u_new = (u - tau div) + shrinkage step along g.
+// The step t needs no divergence; primal_step / primal_apply are the two halves, so a kernel can
+// compute t before the dual that the divergence waits for (the same operations either way).
 template <typename T>
-__device__ __forceinline__ void primal_voxel(const T u[3], const T div[3], float tau, float factor, T rc,
-                                             const T g[3], T un[3]) {
+__device__ __forceinline__ T primal_step(const T u[3], float factor, T rc, const T g[3]) {
   const T rho = vadd(rc, dot3(u[0], u[1], u[2], g[0], g[1], g[2]));
   const T g2s = dot3(g[0], g[1], g[2], g[0], g[1], g[2]);
+  return shrink_step(rho, g2s, factor);
+}
+template <typename T>
+__device__ __forceinline__ void primal_apply(const T u[3], const T div[3], float tau, T t, const T g[3], T un[3]) {
   const T mt = bcast<T>(-tau);
 #pragma unroll
   for (int c = 0; c < 3; ++c) un[c] = vfma(mt, div[c], u[c]);
-  const T t = shrink_step(rho, g2s, factor);
 #pragma unroll
   for (int c = 0; c < 3; ++c) un[c] = vfma(t, g[c], un[c]);
+}
+template <typename T>
+__device__ __forceinline__ void primal_voxel(const T u[3], const T div[3], float tau, float factor, T rc,
+                                             const T g[3], T un[3]) {
+  primal_apply(u, div, tau, primal_step(u, factor, rc, g), g, un);
 }
 
 // div = (dx + dy) + dz
@@ -870,20 +879,26 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
       dxy[c] = vadd(dx, apply3<GEN>(ay, dn, oy, up));
     }
   };
-  // primal of plane j: qn = q_z(j+1), uj = own u at plane j
-  auto finish_primal = [&](int j, const T (&dxy)[3], const T (&qn)[3], const T (&uj)[3]) {
+  // primal of plane j, the part that needs no new dual (run before the dual of plane j+1):
+  // own u, the data-term gradient g and the shrinkage step t
+  auto primal_pre = [&](int j, T (&uj)[3], T (&g)[3], T& t) {
     const unsigned char* R = rbox(j);
     const SP* RC = reinterpret_cast<const SP*>(R) + ro;
     const SP* GW = reinterpret_cast<const SP*>(R + B::RC_SLOT) + ro;
-    const StencilV<T> az = bcast_st<T>(adj_coef(j, nz, bdry, ihz));
-    const T rc = Lane<V, SP>::ld(RC);
-    T g[3], d[3], n[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
+      uj[c] = Lane<V, SU>::ld(ubox(j) + uo + c * UC);
       g[c] = Lane<V, SP>::ld(GW + c * RCS);
-      d[c] = vadd(dxy[c], apply3<GEN>(az, qmm[c], qm[c], qn[c]));
     }
-    primal_voxel(uj, d, a.tau, a.factor, rc, g, n);
+    t = primal_step(uj, a.factor, Lane<V, SP>::ld(RC), g);
+  };
+  // rest of the primal of plane j: qn = q_z(j+1)
+  auto finish_primal = [&](int j, const T (&dxy)[3], const T (&qn)[3], const T (&uj)[3], const T (&g)[3], T t) {
+    const StencilV<T> az = bcast_st<T>(adj_coef(j, nz, bdry, ihz));
+    T d[3], n[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) d[c] = vadd(dxy[c], apply3<GEN>(az, qmm[c], qm[c], qn[c]));
+    primal_apply(uj, d, a.tau, t, g, n);
     SU* dst = u_dst + (long long)j * plane;
     if (full) {
 #pragma unroll
@@ -923,14 +938,17 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
     // coefficient for them is zero (every boundary type): plane k stands in for them
     const SU* Um = ubox(k - 1 >= pl ? k - 1 : k) + uo;
     const SU* Up = ubox(k + 1 <= ph ? k + 1 : k) + uo;
-    T dxy[3], um[3], qxo[3], qyo[3];
+    T dxy[3], um[3], qxo[3], qyo[3], uo1[3], gp[3], tp;
     float qxs[3];
     if (WP && role == 0) {
       if (AS && !wait_q(k - 1)) {
         bad = true;
         return;
       }
-      if (active && !bad) load_dxy(k - 1, dxy);
+      if (active && !bad) {
+        load_dxy(k - 1, dxy);
+        primal_pre(k - 1, uo1, gp, tp);
+      }
     }
     if (role != 2) {
       if (active && !bad) {
@@ -1011,7 +1029,7 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
       }
     }
     if constexpr (AS) mbar_arrive(qpub + ((k - kb) & 1));
-    if (WP && role == 0 && active && !bad) finish_primal(k - 1, dxy, qc, um);
+    if (WP && role == 0 && active && !bad) finish_primal(k - 1, dxy, qc, uo1, gp, tp);
     if constexpr (AS) {
       mbar_arrive(freed + (k - kb) % G::NFR);
     } else {
@@ -1058,12 +1076,11 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
       return;
     }
     if (role == 0 && active && j >= z0) {
-      T dxy[3], uj[3];
+      T dxy[3], uj[3], g[3], t;
       const T zero[3] = {bcast<T>(0.f), bcast<T>(0.f), bcast<T>(0.f)};
-#pragma unroll
-      for (int c = 0; c < 3; ++c) uj[c] = Lane<V, SU>::ld(ubox(j) + uo + c * UC);
       load_dxy(j, dxy);
-      finish_primal(j, dxy, zero, uj);
+      primal_pre(j, uj, g, t);
+      finish_primal(j, dxy, zero, uj, g, t);
     }
   }
 }
