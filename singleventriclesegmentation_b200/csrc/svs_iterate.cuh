@@ -938,98 +938,129 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
     // coefficient for them is zero (every boundary type): plane k stands in for them
     const SU* Um = ubox(k - 1 >= pl ? k - 1 : k) + uo;
     const SU* Up = ubox(k + 1 <= ph ? k + 1 : k) + uo;
-    T dxy[3], um[3], qxo[3], qyo[3], uo1[3], gp[3], tp;
-    float qxs[3];
-    if (WP && role == 0) {
-      if (AS && !wait_q(k - 1)) {
+    if (role == 0) {
+      // interior lanes, one block with few branches so that the compiler can interleave the
+      // primal of plane k-1 with the dual of plane k; lanes outside the volume compute on the
+      // zero fill of the boxes (finite values) and store nothing to global memory
+      T dxy[3], uo1[3], gp[3], tp;
+      if constexpr (WP) {
+        if (AS && !wait_q(k - 1)) {
+          bad = true;
+          return;
+        }
+        load_dxy(k - 1, dxy);
+        primal_pre(k - 1, uo1, gp, tp);
+      }
+      const StencilV<T> fz = bcast_st<T>(fz1);
+      const SP* P = reinterpret_cast<const SP*>(PD) + po;
+      const SP* Dm = reinterpret_cast<const SP*>(PD + B::P_SLOT) + po;
+      T pk[9], Dk[6], qxo[3], qyo[3];
+#pragma unroll
+      for (int c = 0; c < 9; ++c) pk[c] = Lane<V, SP>::ld(P + c * PC);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) Dk[c] = Lane<V, SP>::ld(Dm + c * PC);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const SU* u = Uk + c * UC;
+        const T o = Lane<V, SU>::ld(u);
+        const T ex = apply3<GEN>(fx, prev_x(Store<SU>::sh(u - 1), o), o, next_x(o, Store<SU>::sh(u + V)));
+        const T ey = apply3<GEN>(fy, Lane<V, SU>::ld(u - UXB), o, Lane<V, SU>::ld(u + UXB));
+        const T ez = apply3<GEN>(fz, Lane<V, SU>::ld(Um + c * UC), o, Lane<V, SU>::ld(Up + c * UC));
+        dual_row(Dk, ex, ey, ez, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2], a.sigma, a.wtv, wtv2);
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const T* pc = &pk[3 * c];
+        qyo[c] = dot3(Dk[1], Dk[3], Dk[4], pc[0], pc[1], pc[2]);
+        qxo[c] = dot3(Dk[0], Dk[1], Dk[2], pc[0], pc[1], pc[2]);
+        qc[c] = dot3(Dk[2], Dk[4], Dk[5], pc[0], pc[1], pc[2]);
+      }
+      if (active && !bad && k >= z0 && k < z1) {
+        SP* dst = p_dst + (long long)k * plane;
+        if (full) {
+#pragma unroll
+          for (int c = 0; c < 9; ++c) Lane<V, SP>::st(dst + c * cs, pk[c]);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 9; ++c) Store<SP>::st(dst + c * cs, first(pk[c]));
+        }
+      }
+      // AS: the q slot of plane k was last read by the primal of plane k-2 (step k-1)
+      if (AS && k > kb && !wait_free(k - 1)) {
+        bad = true;
+        return;
+      }
+      // cells outside the volume keep their zeros
+      const T zero = bcast<T>(0.f);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        Lane<V, float>::st(&sqy[qs][c][ly + 1][lx], active ? qyo[c] : zero);
+        Lane<V, float>::st(&sqx[qs][c][ly][lx + 2], active ? qxo[c] : zero);
+      }
+      if constexpr (AS) mbar_arrive(qpub + ((k - kb) & 1));
+      if (WP && active && !bad) finish_primal(k - 1, dxy, qc, uo1, gp, tp);
+    } else {
+      T qyo[3];
+      float qxs[3];
+      if (role == 1) {
+        if (active && !bad) {
+          const StencilV<T> fz = bcast_st<T>(fz1);
+          const SP* P = reinterpret_cast<const SP*>(PD) + po;
+          const SP* Dm = reinterpret_cast<const SP*>(PD + B::P_SLOT) + po;
+          T pk[9], Dk[6];
+#pragma unroll
+          for (int c = 0; c < 9; ++c) pk[c] = Lane<V, SP>::ld(P + c * PC);
+#pragma unroll
+          for (int c = 0; c < 6; ++c) Dk[c] = Lane<V, SP>::ld(Dm + c * PC);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const SU* u = Uk + c * UC;
+            const T o = Lane<V, SU>::ld(u);
+            const T ex = apply3<GEN>(fx, prev_x(Store<SU>::sh(u - 1), o), o, next_x(o, Store<SU>::sh(u + V)));
+            const T ey = apply3<GEN>(fy, Lane<V, SU>::ld(u - UXB), o, Lane<V, SU>::ld(u + UXB));
+            const T ez = apply3<GEN>(fz, Lane<V, SU>::ld(Um + c * UC), o, Lane<V, SU>::ld(Up + c * UC));
+            dual_row(Dk, ex, ey, ez, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2], a.sigma, a.wtv, wtv2);
+          }
+#pragma unroll
+          for (int c = 0; c < 3; ++c) qyo[c] = dot3(Dk[1], Dk[3], Dk[4], pk[3 * c], pk[3 * c + 1], pk[3 * c + 2]);
+        }
+      } else if (active && !bad) {
+        // halo column: one voxel, scalar arithmetic
+        const SP* P = reinterpret_cast<const SP*>(PD) + po;
+        const SP* Dm = reinterpret_cast<const SP*>(PD + B::P_SLOT) + po;
+        float pk[9], Dk[6];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) pk[c] = Store<SP>::sh(P + c * PC);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) Dk[c] = Store<SP>::sh(Dm + c * PC);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const SU* u = Uk + c * UC;
+          const float o = Store<SU>::sh(u);
+          const float ex = apply3<GEN>(fx0, Store<SU>::sh(u - 1), o, Store<SU>::sh(u + 1));
+          const float ey = apply3<GEN>(fy1, Store<SU>::sh(u - UXB), o, Store<SU>::sh(u + UXB));
+          const float ez = apply3<GEN>(fz1, Store<SU>::sh(Um + c * UC), o, Store<SU>::sh(Up + c * UC));
+          dual_row(Dk, ex, ey, ez, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2], a.sigma, a.wtv, wtv2);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) qxs[c] = dot3(Dk[0], Dk[1], Dk[2], pk[3 * c], pk[3 * c + 1], pk[3 * c + 2]);
+      }
+      // AS: the q slot of plane k was last read by the primal of plane k-2 (step k-1)
+      if (AS && k > kb && !wait_free(k - 1)) {
         bad = true;
         return;
       }
       if (active && !bad) {
-        load_dxy(k - 1, dxy);
-        primal_pre(k - 1, uo1, gp, tp);
-      }
-    }
-    if (role != 2) {
-      if (active && !bad) {
-        const StencilV<T> fz = bcast_st<T>(fz1);
-        const SP* P = reinterpret_cast<const SP*>(PD) + po;
-        const SP* Dm = reinterpret_cast<const SP*>(PD + B::P_SLOT) + po;
-        T pk[9], Dk[6];
+        if (role == 2) {
 #pragma unroll
-        for (int c = 0; c < 9; ++c) pk[c] = Lane<V, SP>::ld(P + c * PC);
+          for (int c = 0; c < 3; ++c) sqx[qs][c][ly][lx + 2] = qxs[c];
+        } else {
 #pragma unroll
-        for (int c = 0; c < 6; ++c) Dk[c] = Lane<V, SP>::ld(Dm + c * PC);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const SU* u = Uk + c * UC;
-          const T o = Lane<V, SU>::ld(u);
-          um[c] = Lane<V, SU>::ld(Um + c * UC);
-          const T ex = apply3<GEN>(fx, prev_x(Store<SU>::sh(u - 1), o), o, next_x(o, Store<SU>::sh(u + V)));
-          const T ey = apply3<GEN>(fy, Lane<V, SU>::ld(u - UXB), o, Lane<V, SU>::ld(u + UXB));
-          const T ez = apply3<GEN>(fz, um[c], o, Lane<V, SU>::ld(Up + c * UC));
-          dual_row(Dk, ex, ey, ez, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2], a.sigma, a.wtv, wtv2);
-        }
-        if (role == 0 && k >= z0 && k < z1) {
-          SP* dst = p_dst + (long long)k * plane;
-          if (full) {
-#pragma unroll
-            for (int c = 0; c < 9; ++c) Lane<V, SP>::st(dst + c * cs, pk[c]);
-          } else {
-#pragma unroll
-            for (int c = 0; c < 9; ++c) Store<SP>::st(dst + c * cs, first(pk[c]));
-          }
-        }
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const T* pc = &pk[3 * c];
-          qyo[c] = dot3(Dk[1], Dk[3], Dk[4], pc[0], pc[1], pc[2]);
-          if (role == 0) {
-            qxo[c] = dot3(Dk[0], Dk[1], Dk[2], pc[0], pc[1], pc[2]);
-            qc[c] = dot3(Dk[2], Dk[4], Dk[5], pc[0], pc[1], pc[2]);
-          }
+          for (int c = 0; c < 3; ++c) Lane<V, float>::st(&sqy[qs][c][ly + 1][lx], qyo[c]);
         }
       }
-    } else if (active && !bad) {
-      // halo column: one voxel, scalar arithmetic
-      const SP* P = reinterpret_cast<const SP*>(PD) + po;
-      const SP* Dm = reinterpret_cast<const SP*>(PD + B::P_SLOT) + po;
-      float pk[9], Dk[6];
-#pragma unroll
-      for (int c = 0; c < 9; ++c) pk[c] = Store<SP>::sh(P + c * PC);
-#pragma unroll
-      for (int c = 0; c < 6; ++c) Dk[c] = Store<SP>::sh(Dm + c * PC);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const SU* u = Uk + c * UC;
-        const float o = Store<SU>::sh(u);
-        const float ex = apply3<GEN>(fx0, Store<SU>::sh(u - 1), o, Store<SU>::sh(u + 1));
-        const float ey = apply3<GEN>(fy1, Store<SU>::sh(u - UXB), o, Store<SU>::sh(u + UXB));
-        const float ez = apply3<GEN>(fz1, Store<SU>::sh(Um + c * UC), o, Store<SU>::sh(Up + c * UC));
-        dual_row(Dk, ex, ey, ez, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2], a.sigma, a.wtv, wtv2);
-      }
-#pragma unroll
-      for (int c = 0; c < 3; ++c) qxs[c] = dot3(Dk[0], Dk[1], Dk[2], pk[3 * c], pk[3 * c + 1], pk[3 * c + 2]);
+      if constexpr (AS) mbar_arrive(qpub + ((k - kb) & 1));
     }
-    // AS: the q slot of plane k was last read by the primal of plane k-2 (step k-1)
-    if (AS && k > kb && !wait_free(k - 1)) {
-      bad = true;
-      return;
-    }
-    if (active && !bad) {
-      if (role == 2) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) sqx[qs][c][ly][lx + 2] = qxs[c];
-      } else {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          Lane<V, float>::st(&sqy[qs][c][ly + 1][lx], qyo[c]);
-          if (role == 0) Lane<V, float>::st(&sqx[qs][c][ly][lx + 2], qxo[c]);
-        }
-      }
-    }
-    if constexpr (AS) mbar_arrive(qpub + ((k - kb) & 1));
-    if (WP && role == 0 && active && !bad) finish_primal(k - 1, dxy, qc, uo1, gp, tp);
     if constexpr (AS) {
       mbar_arrive(freed + (k - kb) % G::NFR);
     } else {
