@@ -4,7 +4,8 @@
 // Data layout in HBM (per pair and pyramid level, n = NZ*NY*NX voxels): every field is PLANAR
 // (component-major: comp c of voxel v at [c*n + v]) so that a warp's 32 consecutive x-voxels
 // read 32 consecutive elements of each component.
-//   float : I0, I1 (level images), g1 = grad I1 (3 planes)
+//   float : I0, I1 (level images), ig = (I1, grad I1) interleaved, one float4 per voxel (the
+//           four fields the linearisation samples at the same 64 taps, one 16-byte load each)
 //   S     : D (6 planes, the symmetric anisotropic tensor s n n^T + t1 t1^T packed
 //           d00 d01 d02 d11 d12 d22), rc (rho_c), gw (warped gradient, 3 planes),
 //           u[2] (3 planes each, ping-pong), p[2] (9 planes each, ping-pong)
@@ -120,7 +121,8 @@ __global__ void restrict_kernel(const Desc* __restrict__ fine, const Desc* __res
   const_cast<float*>(c.I1)[v] = sample(r1, cz, cy, cx, f.hz, f.hy, f.hx, interp, bdry);
 }
 
-// Per-level preparation, tvl13d.py:179-192: g1 = grad I1 (differentialOps.cu:540-655), the
+// Per-level preparation, tvl13d.py:179-192: grad I1 (differentialOps.cu:540-655), stored with I1
+// as one float4 per voxel, the
 // anisotropic tensor from s, n, t1 (anisotropicDifferentialOps.cu:89-141) packed as the
 // symmetric matrix s n n^T + t1 t1^T (d00 d01 d02 d11 d12 d22), and (first level only) zero u, p.
 // Without anisotropy D is the identity (tvl13d.py:218-219, 231-232 skip the operator).
@@ -137,9 +139,7 @@ __global__ void prepare_kernel(const Desc* __restrict__ descs, int use_aniso, fl
   const float g0 = fwd_axis(x > 0 ? I[v - 1] : 0.f, c, x < d.nx - 1 ? I[v + 1] : 0.f, x, d.nx, bdry, d.hx);
   const float g1 = fwd_axis(y > 0 ? I[v - sy] : 0.f, c, y < d.ny - 1 ? I[v + sy] : 0.f, y, d.ny, bdry, d.hy);
   const float g2 = fwd_axis(z > 0 ? I[v - sz] : 0.f, c, z < d.nz - 1 ? I[v + sz] : 0.f, z, d.nz, bdry, d.hz);
-  d.g1[v] = g0;
-  d.g1[d.n + v] = g1;
-  d.g1[2 * d.n + v] = g2;
+  reinterpret_cast<float4*>(d.ig)[v] = make_float4(c, g0, g1, g2);
   float D[6] = {1.f, 0.f, 0.f, 1.f, 0.f, 1.f};
   if (use_aniso) {
     const float norm = sqrtf(g0 * g0 + g1 * g1 + g2 * g2);
@@ -171,11 +171,11 @@ __global__ void prepare_kernel(const Desc* __restrict__ descs, int use_aniso, fl
   }
 }
 
-// Tricubic sample of four fields (I1 and the 3 planes of grad I1) at one coordinate, sharing
-// the folded indices (warpingOps.cu:572-596 and :632-660 recompute them per component).
-__device__ __forceinline__ void sample_cubic4(const float* __restrict__ I, const float* __restrict__ G,
-                                              int64_t n, int nz, int ny, int nx, float cz, float cy,
-                                              float cx, float hz, float hy, float hx, int bdry,
+// Tricubic sample of four interleaved fields (I1 and grad I1, one float4 per voxel) at one
+// coordinate, one 16-byte load per tap (warpingOps.cu:572-596 and :632-660 sample each field
+// separately, with the same weights and order).
+__device__ __forceinline__ void sample_cubic4(const float4* __restrict__ IG, int nz, int ny, int nx, float cz,
+                                              float cy, float cx, float hz, float hy, float hx, int bdry,
                                               float out[4]) {
   int ix, iy, iz;
   float wx, wy, wz;
@@ -195,13 +195,12 @@ __device__ __forceinline__ void sample_cubic4(const float* __restrict__ I, const
     float by[4][4];
 #pragma unroll
     for (int dy = 0; dy < 4; ++dy) {
-      const int64_t row = ((int64_t)zz * ny + ys[dy]) * nx;
-#pragma unroll
-      for (int f = 0; f < 4; ++f) {
-        const float* F = (f == 0) ? I : G + (f - 1) * n;
-        by[f][dy] = hermite4(__ldg(F + row + xs[0]), __ldg(F + row + xs[1]), __ldg(F + row + xs[2]),
-                             __ldg(F + row + xs[3]), wx);
-      }
+      const float4* R = IG + ((int64_t)zz * ny + ys[dy]) * nx;
+      const float4 t0 = __ldg(R + xs[0]), t1 = __ldg(R + xs[1]), t2 = __ldg(R + xs[2]), t3 = __ldg(R + xs[3]);
+      by[0][dy] = hermite4(t0.x, t1.x, t2.x, t3.x, wx);
+      by[1][dy] = hermite4(t0.y, t1.y, t2.y, t3.y, wx);
+      by[2][dy] = hermite4(t0.z, t1.z, t2.z, t3.z, wx);
+      by[3][dy] = hermite4(t0.w, t1.w, t2.w, t3.w, wx);
     }
 #pragma unroll
     for (int f = 0; f < 4; ++f) bz[f][dz] = hermite4(by[f][0], by[f][1], by[f][2], by[f][3], wy);
@@ -226,10 +225,10 @@ __global__ void linearise_kernel(const Desc* __restrict__ descs, int src, int in
   const float cz = (float)z * d.hz + u2;
   float s[4];
   if (interp == SVS_INTERPOLATE_CUBIC_HERMITESPLINE) {
-    sample_cubic4(d.I1, d.g1, d.n, d.nz, d.ny, d.nx, cz, cy, cx, d.hz, d.hy, d.hx, bdry, s);
+    sample_cubic4(reinterpret_cast<const float4*>(d.ig), d.nz, d.ny, d.nx, cz, cy, cx, d.hz, d.hy, d.hx, bdry, s);
   } else {
     for (int f = 0; f < 4; ++f) {
-      FieldRef r{f == 0 ? d.I1 : d.g1 + (f - 1) * d.n, d.nz, d.ny, d.nx, 1};
+      FieldRef r{d.ig + f, d.nz, d.ny, d.nx, 4};
       s[f] = sample(r, cz, cy, cx, d.hz, d.hy, d.hx, interp, bdry);
     }
   }
@@ -311,6 +310,109 @@ __global__ void prolong_kernel(const Desc* __restrict__ coarse, const Desc* __re
     } else {
       Store<SP>::st(pf + (comp - 3) * f.cs + of, val);
     }
+  }
+}
+
+// Cubic coarse -> fine transfer as three separable passes through shared memory: x (reading the
+// coarse field), then y, then z. Every output is the same nesting of hermite4 calls on the same
+// values as in prolong_kernel (x innermost, then y, then z; folded tap indices), so the result is
+// bitwise the same, but a block of PFX x PFY x PFZ fine voxels reads each coarse value it needs
+// about once per component instead of 64 times per output. Valid when every coarse axis has at
+// most as many nodes as the fine one (the pyramid's halving): a block then needs at most PF + 4
+// coarse rows per axis.
+constexpr int PFX = 32, PFY = 8, PFZ = 8;
+template <typename SU, typename SP>
+__global__ void __launch_bounds__(PFX * PFY)
+prolong_cubic_kernel(const Desc* __restrict__ coarse, const Desc* __restrict__ fine, int src, int bdry) {
+  __shared__ float A[PFZ + 4][PFY + 4][PFX];  // x pass at coarse (z, y) rows
+  __shared__ float Bz[PFZ + 4][PFY][PFX];     // y pass at coarse z rows
+  __shared__ int tix[PFX], tiy[PFY], tiz[PFZ];
+  __shared__ float twx[PFX], twy[PFY], twz[PFZ];
+  const Desc c = coarse[blockIdx.y], f = fine[blockIdx.y];
+  const int nbx = (f.nx + PFX - 1) / PFX, nby = (f.ny + PFY - 1) / PFY, nbz = (f.nz + PFZ - 1) / PFZ;
+  if ((int)blockIdx.x >= nbx * nby * nbz) return;
+  const int x0 = (blockIdx.x % nbx) * PFX, y0 = ((blockIdx.x / nbx) % nby) * PFY, z0 = (blockIdx.x / (nbx * nby)) * PFZ;
+  const int nxb = min(PFX, f.nx - x0), nyb = min(PFY, f.ny - y0), nzb = min(PFZ, f.nz - z0);
+  const int tid = threadIdx.x;
+  // per-axis taps and weights of the block's fine nodes, as prolong_kernel computes them
+  if (tid < PFX) {
+    float w = 0.f;
+    int i = 0;
+    if (tid < nxb) split_coord((float)(x0 + tid) * f.hx * c.lx / f.lx, c.hx, i, w);
+    tix[tid] = i;
+    twx[tid] = w;
+  } else if (tid < PFX + PFY) {
+    const int k = tid - PFX;
+    float w = 0.f;
+    int i = 0;
+    if (k < nyb) split_coord((float)(y0 + k) * f.hy * c.ly / f.ly, c.hy, i, w);
+    tiy[k] = i;
+    twy[k] = w;
+  } else if (tid < PFX + PFY + PFZ) {
+    const int k = tid - PFX - PFY;
+    float w = 0.f;
+    int i = 0;
+    if (k < nzb) split_coord((float)(z0 + k) * f.hz * c.lz / f.lz, c.hz, i, w);
+    tiz[k] = i;
+    twz[k] = w;
+  }
+  __syncthreads();
+  // coarse rows the block needs: [i(first) - 1, i(last) + 2] per axis (taps are monotone in the
+  // fine index); at most PF + 4 rows when the coarse axis is no finer than the fine one
+  const int ylo = tiy[0] - 1, zlo = tiz[0] - 1;
+  const int nyr = min(tiy[nyb - 1] + 3 - ylo, PFY + 4), nzr = min(tiz[nzb - 1] + 3 - zlo, PFZ + 4);
+  const float kx = (float)((double)f.lx / (double)c.lx);
+  const float ky = (float)((double)f.ly / (double)c.ly);
+  const float kz = (float)((double)f.lz / (double)c.lz);
+  const SU* uc = reinterpret_cast<const SU*>(c.u[src]);
+  const SP* pc = reinterpret_cast<const SP*>(c.p[src]);
+  SU* uf = reinterpret_cast<SU*>(f.u[0]);
+  SP* pf = reinterpret_cast<SP*>(f.p[0]);
+  const int xf = tid % PFX, yf = tid / PFX;
+  for (int comp = 0; comp < 12; ++comp) {
+    const SU* FU = uc + comp * c.cs;
+    const SP* FP = pc + (comp - 3) * c.cs;
+    // x pass: A[z row][y row][fine x]
+    for (int e = tid; e < nzr * nyr * PFX; e += PFX * PFY) {
+      const int xi = e % PFX, yr = (e / PFX) % nyr, zr = e / (PFX * nyr);
+      if (xi >= nxb) continue;
+      const int zz = fold(zlo + zr, c.nz, bdry), yy = fold(ylo + yr, c.ny, bdry);
+      const long long row = pidx(c, zz, yy, 0);
+      const int ix = tix[xi];
+      long long o[4];
+#pragma unroll
+      for (int d = 0; d < 4; ++d) o[d] = row + fold(ix + d - 1, c.nx, bdry);
+      float v[4];
+      if (comp < 3) {
+#pragma unroll
+        for (int d = 0; d < 4; ++d) v[d] = Store<SU>::ld(FU + o[d]);
+      } else {
+#pragma unroll
+        for (int d = 0; d < 4; ++d) v[d] = Store<SP>::ld(FP + o[d]);
+      }
+      A[zr][yr][xi] = hermite4(v[0], v[1], v[2], v[3], twx[xi]);
+    }
+    __syncthreads();
+    // y pass: Bz[z row][fine y][fine x]
+    for (int e = tid; e < nzr * PFY * PFX; e += PFX * PFY) {
+      const int xi = e % PFX, yi = (e / PFX) % PFY, zr = e / (PFX * PFY);
+      if (xi >= nxb || yi >= nyb) continue;
+      const int r = tiy[yi] - 1 - ylo;
+      Bz[zr][yi][xi] = hermite4(A[zr][r][xi], A[zr][r + 1][xi], A[zr][r + 2][xi], A[zr][r + 3][xi], twy[yi]);
+    }
+    __syncthreads();
+    // z pass and store: thread (yf, xf) writes its column of the block
+    if (xf < nxb && yf < nyb) {
+      const float k = comp == 0 ? kx : (comp == 1 ? ky : kz);
+      for (int zi = 0; zi < nzb; ++zi) {
+        const int r = tiz[zi] - 1 - zlo;
+        const float val = hermite4(Bz[r][yf][xf], Bz[r + 1][yf][xf], Bz[r + 2][yf][xf], Bz[r + 3][yf][xf], twz[zi]);
+        const long long of = pidx(f, z0 + zi, y0 + yf, x0 + xf);
+        if (comp < 3) Store<SU>::st(uf + comp * f.cs + of, val * k);
+        else Store<SP>::st(pf + (comp - 3) * f.cs + of, val);
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -843,6 +945,26 @@ svs_status setup_tiles(svs_plan& P) {
   return check_cuda(cudaMemcpy(P.d_maps, maps.data(), maps.size() * sizeof(TMaps), cudaMemcpyHostToDevice), "tensor maps");
 }
 
+// Blocks of prolong_cubic_kernel for the largest pair of a (fine) level.
+unsigned prolong_blocks(const svs_plan& P, int level) {
+  long long m = 0;
+  for (int i = 0; i < P.num_pairs; ++i) {
+    const Desc& d = P.h_descs[(size_t)level * P.num_pairs + i];
+    m = std::max(m, (long long)ceil_div(d.nx, PFX) * ceil_div(d.ny, PFY) * ceil_div(d.nz, PFZ));
+  }
+  return (unsigned)m;
+}
+
+// Every pair's level `level` has at most as many nodes per axis as level-1 (prolong_cubic_kernel).
+bool coarse_within(const svs_plan& P, int level) {
+  for (int i = 0; i < P.num_pairs; ++i) {
+    const Desc& c = P.h_descs[(size_t)level * P.num_pairs + i];
+    const Desc& f = P.h_descs[(size_t)(level - 1) * P.num_pairs + i];
+    if (c.nx > f.nx || c.ny > f.ny || c.nz > f.nz) return false;
+  }
+  return true;
+}
+
 long long max_voxels(const svs_plan& P, int level) {
   long long m = 0;
   for (int i = 0; i < P.num_pairs; ++i) m = std::max(m, P.h_descs[(size_t)level * P.num_pairs + i].n);
@@ -935,7 +1057,12 @@ long long enqueue_solve(svs_plan& P, cudaStream_t s) {
       }
     }
     if (l > 0) {
-      prolong_kernel<SU, SP><<<grid(l - 1), 256, 0, s>>>(D + (size_t)l * np, D + (size_t)(l - 1) * np, cur, q.interpolation, q.boundary);
+      if (q.interpolation == SVS_INTERPOLATE_CUBIC_HERMITESPLINE && coarse_within(P, l))
+        prolong_cubic_kernel<SU, SP><<<dim3(prolong_blocks(P, l - 1), np), PFX * PFY, 0, s>>>(
+            D + (size_t)l * np, D + (size_t)(l - 1) * np, cur, q.boundary);
+      else
+        prolong_kernel<SU, SP><<<grid(l - 1), 256, 0, s>>>(D + (size_t)l * np, D + (size_t)(l - 1) * np, cur,
+                                                          q.interpolation, q.boundary);
       ++launches;
       cur = 0;
     }
@@ -1034,7 +1161,7 @@ svs_status svs_tvl1_plan_create(const svs_tvl1_params* prm, int num_pairs, const
       else { d.lz = prm->length_z; d.ly = prm->length_y; d.lx = prm->length_x; }
       d.hz = d.lz / (float)(nz - 1); d.hy = d.ly / (float)(ny - 1); d.hx = d.lx / (float)(nx - 1);
       const size_t n = (size_t)d.n, cs = (size_t)d.cs;
-      bytes += 2 * al(n * 4) + al(3 * n * 4);                       // I0, I1, g1
+      bytes += 2 * al(n * 4) + al(4 * n * 4);                       // I0, I1, ig
       bytes += al(6 * cs * sb) + al(cs * sb) + al(3 * cs * sb);      // D, rc, gw
       bytes += 2 * al(3 * cs * ub) + 2 * al(9 * cs * sb);            // u[2], p[2]
       if (9 * cs >= (size_t)1 << 31) { delete P; return fail(SVS_ERR_INVALID_ARG, "svs_tvl1_plan_create: volume too large for 32-bit field offsets"); }
@@ -1057,7 +1184,7 @@ svs_status svs_tvl1_plan_create(const svs_tvl1_params* prm, int num_pairs, const
       const size_t n = (size_t)d.n, cs = (size_t)d.cs;
       d.I0 = carve<float>(cur, n);
       d.I1 = carve<float>(cur, n);
-      d.g1 = carve<float>(cur, 3 * n);
+      d.ig = carve<float>(cur, 4 * n);
       d.D = carve<char>(cur, 6 * cs * sb);
       d.rc = carve<char>(cur, cs * sb);
       d.gw = carve<char>(cur, 3 * cs * sb);
@@ -1444,7 +1571,7 @@ extern "C" svs_status svs_tvl1_solve_noalloc(const svs_tvl1_params* prm, const f
       else { d.lz = prm->length_z; d.ly = prm->length_y; d.lx = prm->length_x; }
       d.hz = d.lz / (float)(z - 1); d.hy = d.ly / (float)(y - 1); d.hx = d.lx / (float)(x - 1);
       const size_t n = (size_t)d.n, cs = (size_t)d.cs;
-      bytes += 2 * al(n * 4) + al(3 * n * 4) + al(6 * cs * sb) + al(cs * sb) + al(3 * cs * sb) +
+      bytes += 2 * al(n * 4) + al(4 * n * 4) + al(6 * cs * sb) + al(cs * sb) + al(3 * cs * sb) +
                2 * al(3 * cs * ub) + 2 * al(9 * cs * sb);
       if (l == 0 && prm->median_kernel > 1) bytes += al(3 * n * 4);
     }
@@ -1480,7 +1607,7 @@ extern "C" svs_status svs_tvl1_solve_noalloc(const svs_tvl1_params* prm, const f
     const size_t n = (size_t)d.n, cs = (size_t)d.cs;
     d.I0 = carve<float>(cur, n);
     d.I1 = carve<float>(cur, n);
-    d.g1 = carve<float>(cur, 3 * n);
+    d.ig = carve<float>(cur, 4 * n);
     d.D = carve<char>(cur, 6 * cs * sb);
     d.rc = carve<char>(cur, cs * sb);
     d.gw = carve<char>(cur, 3 * cs * sb);

@@ -56,7 +56,8 @@ template <> struct Pair<__half> {
 };
 
 // One (pair, level) of the batch.
-// Float fields (I0, I1, g1 planes) are dense [nz][ny][nx]. Iteration-state fields of storage
+// Float fields are dense [nz][ny][nx]: I0, I1, and ig = (I1, dI1/dx, dI1/dy, dI1/dz) as one
+// float4 per voxel (16-byte aligned). Iteration-state fields of storage
 // type S (D, rc, gw, u[2], p[2]) are planar and PITCHED: component c of voxel (z, y, x) is at
 // c*cs + (z*ny + y)*pitch + x, with pitch a multiple of 8 elements so that every row starts on a
 // 16-byte boundary (the TMA stride rule) for f32, bf16 and f16 alike.
@@ -68,7 +69,7 @@ struct Desc {
   long long cs;  // component stride of the pitched fields, = pitch * ny * nz
   const float* I0;
   const float* I1;
-  float* g1;
+  float* ig;
   void* D;
   void* rc;
   void* gw;
