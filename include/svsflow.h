@@ -269,6 +269,12 @@ int svs_tvl1_plan_level_tile(const svs_plan* plan, int level);
 /* CTAs of one iteration at a pyramid level, all variant groups together (after the first solve;
  * 0 before): the column tiles times their z chunks. */
 int64_t svs_tvl1_plan_level_ctas(const svs_plan* plan, int level);
+/* The z-chunk plan of the split-role kernels (host arithmetic only, no device needed): for
+ * `columns` column tiles of up to `nz` planes on `slots` resident CTAs (SMs x CTAs per SM), the
+ * first columns - tail_columns march in main_chunks chunks each and the last tail_columns in
+ * tail_chunks, minimising waves x (planes per chunk + 3) summed over the two phases. */
+svs_status svs_tvl1_chunk_plan(int64_t columns, int nz, int64_t slots, int* main_chunks, int* tail_chunks,
+                               int64_t* tail_columns);
 /* Synchronous check of the plan's device status: SVS_ERR_TIMEOUT if a bounded pipeline wait
  * inside an iterate kernel gave up (the kernel then returned early and the results of that
  * solve are invalid), SVS_OK otherwise. */

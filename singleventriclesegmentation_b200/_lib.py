@@ -94,6 +94,7 @@ _SIGS = {
     "svs_tvl1_plan_graph_kernels": (ctypes.c_uint64, [c_void_p]),
     "svs_tvl1_plan_level_tile": (c_int, [c_void_p, c_int]),
     "svs_tvl1_plan_level_ctas": (c_int64, [c_void_p, c_int]),
+    "svs_tvl1_chunk_plan": (c_int, [c_int64, c_int, c_int64, c_void_p, c_void_p, c_void_p]),
     "svs_tvl1_plan_check": (c_int, [c_void_p]),
     "svs_tvl1_solve_noalloc": (c_int, [ctypes.POINTER(TVL1Params), c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
 }
@@ -157,3 +158,12 @@ def tile_info(tile_id: int) -> dict:
     check(lib().svs_tvl1_tile_info(int(tile_id), *[ctypes.byref(x) for x in v]))
     return {"tx": v[0].value, "ty": v[1].value, "dist": v[2].value,
             "form": ("plain", "tma", "split")[v[3].value], "lane_voxels": v[4].value}
+
+
+def chunk_plan(columns: int, nz: int, slots: int) -> dict:
+    """z-chunk plan of the split-role kernels for `columns` column tiles of up to `nz` planes on
+    `slots` resident CTAs: {"main_chunks", "tail_chunks", "tail_columns"} (host arithmetic)."""
+    m, t, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int64()
+    check(lib().svs_tvl1_chunk_plan(int(columns), int(nz), int(slots), ctypes.byref(m), ctypes.byref(t),
+                                    ctypes.byref(c)))
+    return {"main_chunks": m.value, "tail_chunks": t.value, "tail_columns": c.value}

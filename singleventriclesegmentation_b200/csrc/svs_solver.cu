@@ -778,21 +778,10 @@ struct ChunkPlan {
   int main_c = 1, tail_c = 1;
   long long tail_cols = 0;  // the last tail_cols columns of the tile list use tail_c
 };
-ChunkPlan split_chunks(const svs_plan& P, int level, int tid, long long xy_tiles) {
+// The plan for `xy_tiles` columns of up to `nz` planes on `slots` resident CTA slots.
+ChunkPlan chunk_plan(long long xy_tiles, int nz, long long slots) {
   ChunkPlan best;
-  int dev = 0, sms = 148, per_sm = 0, nz = 1;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  int box[4] = {0, 0, 0, 0};
-  const TileShape& ts = kTileShapes[tid - 1];
-  if (!split_variant(P.prm.storage, ts.split, 2, P.prm.boundary != SVS_BOUNDARY_MIRROR, 0, nullptr, nullptr,
-                     nullptr, nullptr, nullptr, nullptr, box) ||
-      xy_tiles <= 0)
-    return best;
-  per_sm = std::max(1, box[0]);
-  for (int i = 0; i < P.num_pairs; ++i)
-    if (!P.pair_mask || (*P.pair_mask)[i]) nz = std::max(nz, P.h_descs[(size_t)level * P.num_pairs + i].nz);
-  const long long slots = (long long)sms * per_sm;
+  if (xy_tiles <= 0 || nz <= 0 || slots <= 0) return best;
   long long best_cost = -1;
   for (int cm = 1; cm <= nz; ++cm) {
     // columns whose chunks fill whole waves; the rest form the tail
@@ -809,6 +798,23 @@ ChunkPlan split_chunks(const svs_plan& P, int level, int tid, long long xy_tiles
     }
   }
   return best;
+}
+
+ChunkPlan split_chunks(const svs_plan& P, int level, int tid, long long xy_tiles) {
+  ChunkPlan best;
+  int dev = 0, sms = 148, per_sm = 0, nz = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int box[4] = {0, 0, 0, 0};
+  const TileShape& ts = kTileShapes[tid - 1];
+  if (!split_variant(P.prm.storage, ts.split, 2, P.prm.boundary != SVS_BOUNDARY_MIRROR, 0, nullptr, nullptr,
+                     nullptr, nullptr, nullptr, nullptr, box) ||
+      xy_tiles <= 0)
+    return best;
+  per_sm = std::max(1, box[0]);
+  for (int i = 0; i < P.num_pairs; ++i)
+    if (!P.pair_mask || (*P.pair_mask)[i]) nz = std::max(nz, P.h_descs[(size_t)level * P.num_pairs + i].nz);
+  return chunk_plan(xy_tiles, nz, (long long)sms * per_sm);
 }
 
 // Tiles of the level's pairs (those in P.pair_mask when set) for variant tid, into `out_opt` or
@@ -1465,6 +1471,17 @@ uint64_t svs_tvl1_plan_graph_kernels(const svs_plan* P) { return P ? P->graph_ke
 
 int svs_tvl1_plan_level_tile(const svs_plan* P, int level) {
   return (P && level >= 0 && level < (int)P->level_tile.size()) ? P->level_tile[level] : 0;
+}
+
+svs_status svs_tvl1_chunk_plan(int64_t columns, int nz, int64_t slots, int* main_chunks, int* tail_chunks,
+                               int64_t* tail_columns) {
+  SVS_REQUIRE(columns > 0 && nz > 0 && slots > 0, "svs_tvl1_chunk_plan: columns, nz and slots must be positive");
+  SVS_REQUIRE(main_chunks && tail_chunks && tail_columns, "svs_tvl1_chunk_plan: null output");
+  const ChunkPlan c = chunk_plan(columns, nz, slots);
+  *main_chunks = c.main_c;
+  *tail_chunks = c.tail_c;
+  *tail_columns = c.tail_cols;
+  return SVS_OK;
 }
 
 int64_t svs_tvl1_plan_level_ctas(const svs_plan* P, int level) {

@@ -3,6 +3,8 @@ import ctypes
 import os
 import re
 
+import pytest
+
 from singleventriclesegmentation_b200 import _lib
 from singleventriclesegmentation_b200.build import LIB, build_library
 
@@ -67,3 +69,39 @@ def test_tile_info_lists_every_variant():
     for bad in (0, n + 1):
         with pytest.raises(_lib.SVSError):
             _lib.tile_info(bad)
+
+
+def _plan_cost(columns, nz, slots, p, fill=3):
+    """Makespan in plane steps of a chunk plan, the quantity the plan minimises."""
+    cdiv = lambda a, b: -(-a // b)
+    main = columns - p["tail_columns"]
+    t = cdiv(main * p["main_chunks"], slots) * (cdiv(nz, p["main_chunks"]) + fill) if main else 0
+    if p["tail_columns"]:
+        t += cdiv(p["tail_columns"] * p["tail_chunks"], slots) * (cdiv(nz, p["tail_chunks"]) + fill)
+    return t
+
+
+def test_chunk_plan_of_the_split_kernels():
+    """The z-chunk plan (host arithmetic, no GPU): the 68-pair 80^3 bench level (1360 40x8 columns
+    on 148 SMs x 2 CTAs) marches 1184 whole columns and cuts the last 176 into 5 chunks; level 1
+    (340 columns of 40 planes) cuts 44 tail columns into 6; one pair's level 0 (20 columns, all of
+    them tail) splits every column into 14. Every plan is at least as short as the best uniform
+    chunk count, and the whole-wave columns fill whole waves up to one column's chunks."""
+    cases = {(1360, 80, 296): (1, 5, 176), (340, 40, 296): (1, 6, 44), (20, 80, 296): (1, 14, 20)}
+    for (cols, nz, slots), want in cases.items():
+        p = _lib.chunk_plan(cols, nz, slots)
+        assert (p["main_chunks"], p["tail_chunks"], p["tail_columns"]) == want, (cols, nz, slots, p)
+    for cols in (1, 7, 150, 296, 297, 1000, 1360, 5000):
+        for nz in (3, 20, 40, 80, 128):
+            for slots in (148, 296, 444):
+                p = _lib.chunk_plan(cols, nz, slots)
+                assert 1 <= p["main_chunks"] <= p["tail_chunks"] <= nz
+                assert 0 <= p["tail_columns"] <= cols
+                main = cols - p["tail_columns"]
+                r = (main * p["main_chunks"]) % slots
+                assert r == 0 or r > slots - p["main_chunks"] or p["tail_columns"] == 0
+                best_uniform = min(_plan_cost(cols, nz, slots, {"main_chunks": c, "tail_chunks": c,
+                                                                 "tail_columns": 0}) for c in range(1, nz + 1))
+                assert _plan_cost(cols, nz, slots, p) <= best_uniform
+    with pytest.raises(_lib.SVSError):
+        _lib.chunk_plan(0, 80, 296)
