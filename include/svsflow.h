@@ -141,7 +141,7 @@ svs_status svs_median3d(const float* in, int nz, int ny, int nx, int C, int ks, 
 
 /* FP64 forms of the per-operator entry points above: the same operators, arguments and
  * semantics on double arrays, with double scalars (the reference dispatches float and double,
- * AT_DISPATCH_FLOATING_TYPES in svs/src/*.cu). Used by the double-precision drop-in operators and
+ * AT_DISPATCH_FLOATING_TYPES in the .cu files of svs/src). Used by the double-precision drop-in operators and
  * the FP64 run of the plain solver on the GPU. */
 svs_status svs_nabla3d_forward_f64(const double* b, int nz, int ny, int nx, int C, double hz, double hy,
                                    double hx, int boundary, double* out, svs_stream_t stream);

@@ -914,8 +914,12 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
     return mbar_wait_abort(qpub + (r & 1), (uint32_t)((r >> 1) & 1), abort_flag);
   };
   auto wait_free = [&](int j) {
-    const int r = j - kb;
-    return mbar_wait_abort(freed + r % G::NFR, (uint32_t)((r / G::NFR) & 1), abort_flag);
+    if constexpr (AS) {
+      const int r = j - kb;
+      return mbar_wait_abort(freed + r % G::NFR, (uint32_t)((r / G::NFR) & 1), abort_flag);
+    } else {
+      return true;  // only the decoupled form waits here
+    }
   };
 
   // One plane step; WITH_PRIMAL: role 0 also finishes plane k-1.
@@ -998,7 +1002,9 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
         Lane<V, float>::st(&sqx[qs][c][ly][lx + 2], active ? qxo[c] : zero);
       }
       if constexpr (AS) mbar_arrive(qpub + ((k - kb) & 1));
-      if (WP && active && !bad) finish_primal(k - 1, dxy, qc, uo1, gp, tp);
+      if constexpr (WP) {
+        if (active && !bad) finish_primal(k - 1, dxy, qc, uo1, gp, tp);
+      }
     } else {
       T qyo[3];
       float qxs[3];
