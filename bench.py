@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain-form", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-latency", action="store_true", help="skip the single-pair latency reps")
+    ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-storage sequence solve")
     ap.add_argument("--frames", type=int, default=T_FRAMES)
     ap.add_argument("--workload", default="sequence", choices=["sequence", "uneven", "mixed", "serving", "latency"],
                     help="sequence: 35-frame 80^3 cine sequence (the headline line); uneven: 64 pairs of "
@@ -147,7 +149,16 @@ def profiled_traffic():
 
 
 # ------------------------------------------------------------------------ CPU baselines
-def oracle_sample(threads: int):
+def sequence_pair(frames: int):
+    """The first forward pair (fixed frame 1, moving frame 0) of the benchmark's cine sequence,
+    generated on the host (bitwise the frames the GPU arm generates on the device)."""
+    from singleventriclesegmentation_b200 import synthetic
+    seq = synthetic.cine_sequence(T=frames, shape=SHAPE, seed=0, device="cpu", first=2)
+    a, b = synthetic.sequence_pairs(frames, "forward")[0]
+    return seq[a], seq[b]
+
+
+def oracle_sample(threads: int, pair=None):
     """One bounded sample of the workload on the host with the oracle (C++/OpenMP restatement of
     the reference's path): one 80^3 pair through the full 3-level pyramid with 1 warp of K
     iterations per level. Returns (seconds, extrapolated seconds per full pair, description)."""
@@ -155,7 +166,10 @@ def oracle_sample(threads: int):
     from singleventriclesegmentation_b200 import synthetic
     o.build()
     o.set_threads(threads)
-    I0, I1, _ = synthetic.frame_pair(SHAPE, seed=0)
+    if pair is None:
+        I0, I1, _ = synthetic.frame_pair(SHAPE, seed=0)
+    else:
+        I0, I1 = pair
     # calibrate the iteration count so that the sample is about 15 s of host work: two probes
     # separate the fixed cost (blur, pyramid, linearisation) from the per-iteration cost
     times = []
@@ -170,9 +184,41 @@ def oracle_sample(threads: int):
     o.tvl1_compute(I0, I1, P, dtype=np.float32)
     dt = time.perf_counter() - t0
     full = dt * (15 * 300) / (1 * k)
-    desc = (f"one 80^3 pair, full 3-level pyramid with 1 warp x {k} iterations per level "
+    src = "one 80^3 pair" if pair is None else "the sequence's first forward pair (80^3)"
+    desc = (f"{src}, full 3-level pyramid with 1 warp x {k} iterations per level "
             f"(= {k}/4500 of the iterations), extrapolated linearly to 15 x 300")
     return dt, full, desc
+
+
+def reference_gpu_rate(frames: int):
+    """The reference's own CUDA extension (its sources built for sm_100a by oracle/build_ref.sh),
+    driven by its solver loop (tvl13d.py:122-255, restated call by call in oracle/ref_driver.py)
+    on the sequence's first pair with the full schedule, serial as its processor runs it; timed
+    with CUDA events. Returns a dict, or {"unavailable": why}."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device"}
+        from oracle import ref_driver
+        from oracle.oracle import SolverParams
+        of = ref_driver.load_reference_module()
+    except Exception as e:  # extension not built or not loadable here
+        return {"unavailable": f"{type(e).__name__}: {e}"[:200]}
+    dev = torch.device("cuda", 0)
+    I0, I1 = (torch.from_numpy(x).to(dev) for x in sequence_pair(frames))
+    ref_driver.tvl1_compute(of, I0, I1, SolverParams(max_warps=1, max_outer_iterations=3))  # warm-up
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record(st)
+    ref_driver.tvl1_compute(of, I0, I1, SolverParams())
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    sec = e0.elapsed_time(e1) / 1000.0
+    return {"value": 1.0 / sec, "unit": "pairs/s", "seconds_per_pair": sec,
+            "form": "the reference's CUDA extension (built for sm_100a with -maxrregcount=80; the stock build "
+                    "returns zero flows on B200) under its own per-operator solver loop, FP32, one 80^3 pair of "
+                    "the sequence, full 3 x 15 x 300 schedule"}
 
 
 def reference_arm(args):
@@ -180,12 +226,13 @@ def reference_arm(args):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
+    pair = sequence_pair(args.frames)
     for _ in range(args.warmup):
-        oracle_sample(threads)
+        oracle_sample(threads, pair)
     samples = []
     desc = ""
     for _ in range(args.steps):
-        dt, full, desc = oracle_sample(threads)
+        dt, full, desc = oracle_sample(threads, pair)
         samples.append(full)
     per_pair = statistics.mean(samples)
     value = 1.0 / per_pair
@@ -194,10 +241,14 @@ def reference_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_pair * 1000.0,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "config": config_dict(args, "f32"),
+        "sample": ("each step times a bounded sample of the workload on the host: " + desc +
+                   "; value = 1 / (extrapolated seconds per pair), the rate the 68-pair sequence runs at"),
         "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": "port", "sample": desc},
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": reference_gpu_rate(args.frames),
         "note": ("the reference has no CPU implementation of the solver (processor.py:33-34 requires "
-                 "CUDA); this arm is the oracle's C++/OpenMP restatement of its kernels on all host threads"),
+                 "CUDA); this arm is the oracle's C++/OpenMP restatement of its kernels on all host threads; "
+                 "reference_gpu times the reference's own CUDA extension on the same pair"),
     }
     print(json.dumps(line), flush=True)
 
@@ -265,6 +316,55 @@ def plain_form_rate(dev, seq_dev):
     return {"value": 1.0 / sec, "unit": "pairs/s", "seconds_per_pair": sec,
             "form": "TVL13DOpticalFlow.compute_unfused: per-operator kernels, FP32, one 80^3 pair, full "
                     "3 x 15 x 300 schedule"}
+
+
+def pair_latency(dev, seq, storage: str, reps: int = 20):
+    """Latency of one 80^3 pair alone (the sequence's first forward pair) through
+    TVL13DOpticalFlow.compute: p50/p99 over `reps` repetitions, each timed with CUDA events around
+    the call and a synchronisation."""
+    import torch
+    st = torch.cuda.current_stream(dev)
+    I0, I1 = torch.from_numpy(seq[1]).to(dev), torch.from_numpy(seq[0]).to(dev)
+    solver = _solver(dev, storage)
+    for _ in range(3):
+        solver.compute(I0, I1)
+    torch.cuda.synchronize(dev)
+    out = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        solver.compute(I0, I1)
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        out.append(e0.elapsed_time(e1) / 1000.0)
+    a = np.array(out)
+    return {"p50_s": float(np.percentile(a, 50)), "p99_s": float(np.percentile(a, 99)), "reps": reps,
+            "storage": storage}
+
+
+def fp32_storage_rate(dev, d_seq, pairs, args):
+    """The same sequence solve with every iteration field stored in FP32 (the plain FP32 form of
+    the fused path): pairs/s over 3 timed solves after autotuning, and the level-0 iterate
+    kernel's roofline fraction (136 algorithmic bytes per voxel-iteration)."""
+    import torch
+    solver = _solver(dev, "f32")
+    n = len(pairs)
+    plan = solver.plan_for([SHAPE] * n)
+    if not args.no_autotune:
+        tune_plan(plan, "f32")
+    flows = [torch.empty(SHAPE + (3,), device=dev) for _ in range(n)]
+    I0s, I1s = [d_seq[a] for a, b in pairs], [d_seq[b] for a, b in pairs]
+    ms, clocks = _timed_solves(plan, I0s, I1s, flows, 3, 2, dev)
+    st = torch.cuda.current_stream(dev)
+    it_ms, alg = iterate_roofline(plan, "f32", n * int(np.prod(SHAPE)), st, dev)
+    peak, kind = measured_peaks()
+    out = {"value": n / (ms / 1000.0), "unit": "pairs/s", "ms_per_step": ms, "steps": 3,
+           "what": "the 68 pair solves alone (no mask propagation), FP32 storage of every field",
+           "level_tiles": plan.level_tiles()[:3], "launch_ms": it_ms,
+           "roofline_frac": alg / (it_ms / 1000.0) / 1e9 / peak, "peak_kind": kind, "clocks": clocks}
+    plan.close()
+    solver._plans.clear()
+    return out
 
 
 # ----------------------------------------------------------------- further workloads (1 GPU)
@@ -580,18 +680,20 @@ def main():
         return float(t.item())
 
     clocks = ClockSampler(local)
-    # ----- device-resident timed region
+    # ----- device-resident timed region (an event between steps gives the per-sequence latency)
     launches0 = _lib.launch_count()
     barrier()
     clocks.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev[0].record(stream)
+    for i in range(args.steps):
         chain = step(d_seq, d_masks)
-    e1.record(stream)
+        ev[i + 1].record(stream)
     barrier()
     clock_info = clocks.stop()
+    e0, e1 = ev[0], ev[-1]
     ms = max_over_ranks(e0.elapsed_time(e1))
+    step_s = np.array([ev[i].elapsed_time(ev[i + 1]) / 1000.0 for i in range(args.steps)])
     launches = _lib.launch_count() - launches0
     value = world * n_pairs * args.steps / (ms / 1000.0)
 
@@ -619,12 +721,26 @@ def main():
     achieved = alg_bytes / (it_ms / 1000.0) / 1e9
     traffic_pv = profiled_traffic().get(args.storage)
 
-    # parity summary of this run (masks): Dice/HD of the propagated end masks
+    # the workload's own end metrics (warping.py:245-270): each propagated end mask against the
+    # mask given at that end (two different synthetic annotations, so these are not parity values)
     from singleventriclesegmentation_b200.warping import dice, hausdorff
     fm = (chain[-1, 0, 0] > 0.5).float()
     bm = (chain[-1, 1, 0] > 0.5).float()
     mask_metrics = {"dice_fwd": dice(fm, d_masks[1, 0]), "hd_fwd": hausdorff(fm, d_masks[1, 0]),
-                    "dice_bwd": dice(bm, d_masks[0, 0]), "hd_bwd": hausdorff(bm, d_masks[0, 0])}
+                    "dice_bwd": dice(bm, d_masks[0, 0]), "hd_bwd": hausdorff(bm, d_masks[0, 0]),
+                    "what": "propagated end mask vs the mask given at that end (t=12 and t=0 annotations)"}
+
+    latency = None
+    if rank == 0 and world == 1 and not args.no_latency:
+        latency = {"sequence_68pairs_with_masks": {"p50_s": float(np.percentile(step_s, 50)),
+                                                   "p99_s": float(np.percentile(step_s, 99)),
+                                                   "reps": int(args.steps),
+                                                   "from": "the timed steps above (events between steps)"},
+                   "pair_80cube": pair_latency(dev, seq, args.storage, reps=20)}
+
+    fp32 = None
+    if rank == 0 and world == 1 and not args.no_fp32:
+        fp32 = fp32_storage_rate(dev, d_seq, pairs, args)
 
     plain = None
     if rank == 0 and world == 1 and not args.no_plain_form:
@@ -654,7 +770,8 @@ def main():
                          "kernel": "iterate kernel (fused primal-dual iteration, variant %d), level 0"
                                    % plan.level_tiles()[0],
                          "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": it_ms},
-            "cpu_baseline": cpu, "plain_gpu_form": plain, "clocks": clock_info, "masks": mask_metrics,
+            "cpu_baseline": cpu, "plain_gpu_form": plain, "clocks": clock_info, "latency": latency,
+            "fp32_storage": fp32, "compute_metrics": mask_metrics,
             "graph_kernels_per_solve": plan.graph_kernels,
         }
         print(json.dumps(line), flush=True)

@@ -218,10 +218,10 @@ svs_status svs_tvl1_plan_destroy(svs_plan* plan);
 size_t svs_tvl1_plan_device_bytes(const svs_plan* plan);
 /* Select the iterate-kernel variant (0 = automatic) for later solves; SVS_ERR_INVALID_ARG for an
  * unknown id. Variants 1-5 are TMA pipelines (tile x prefetch distance: 32x8/2, 32x8/3, 64x4/2,
- * 16x16/2, 32x16/2), 6-8 plain-load forms (32x8, 32x4, 16x16), 9-24 split-role TMA pipelines
+ * 16x16/2, 32x16/2), 6-8 plain-load forms (32x8, 32x4, 16x16), 9-27 split-role TMA pipelines
  * (interior, halo-row and halo-column lanes in separate warps; 21-24 synchronise with mbarriers
- * and a producer warp instead of a block-wide barrier per plane; svs_tvl1_tile_info gives each
- * shape). Used by the autotuner. */
+ * and a producer warp instead of a block-wide barrier per plane; 25 and 26 are sized for three
+ * CTAs per SM; svs_tvl1_tile_info gives each shape). Used by the autotuner. */
 svs_status svs_tvl1_plan_set_tile(svs_plan* plan, int tile_id);
 /* Same for one pyramid level only (0 = fall back to the plan-wide choice). */
 svs_status svs_tvl1_plan_set_level_tile(svs_plan* plan, int level, int tile_id);
@@ -276,9 +276,18 @@ int64_t svs_tvl1_plan_level_ctas(const svs_plan* plan, int level);
 svs_status svs_tvl1_chunk_plan(int64_t columns, int nz, int64_t slots, int* main_chunks, int* tail_chunks,
                                int64_t* tail_columns);
 /* Synchronous check of the plan's device status: SVS_ERR_TIMEOUT if a bounded pipeline wait
- * inside an iterate kernel gave up (the kernel then returned early and the results of that
- * solve are invalid), SVS_OK otherwise. */
+ * inside an iterate kernel gave up (the kernel then returned early and the results of the
+ * solves since the last check are invalid), SVS_OK otherwise. The status is cleared once it has
+ * been reported. */
 svs_status svs_tvl1_plan_check(svs_plan* plan);
+/* Test hook for the bounded pipeline waits of the TMA iterate kernels (no counterpart in the
+ * reference): at pyramid `level`, the CTA with launch index `cta` never issues the copies of its
+ * staged plane number `plane` (counted from the first plane it stages), and every pipeline wait
+ * gives up after wait_us microseconds (0 = the default, 2 s). The waiting threads then record
+ * SVS_DEV_TIMEOUT, the CTA waits (bounded) for the copies it did issue and returns, and
+ * svs_tvl1_plan_check reports SVS_ERR_TIMEOUT; the context stays usable. level, cta or plane < 0
+ * switches the stall off (wait_us still applies). */
+svs_status svs_tvl1_plan_set_stall_test(svs_plan* plan, int level, int cta, int plane, uint32_t wait_us);
 
 /* Allocation-free solve of ONE frame pair, for callers that cannot call cudaMalloc: code whose
  * device memory belongs to another allocator (a framework's caching pool that has reserved the
@@ -289,8 +298,11 @@ svs_status svs_tvl1_plan_check(svs_plan* plan);
  * [nz,ny,nx,3]. All other device memory the solve needs (pyramid, linearisation, dual state,
  * descriptors, tile lists) is taken from one static 32 MiB device array that every GPU loading
  * the library holds until exit; a volume whose state does not fit is rejected with
- * SVS_ERR_INVALID_ARG (about 56^3 fits with FP32 storage, larger with 16-bit storage). Calls no
- * cudaMalloc or cudaFree. The first call on a device looks up the array's device address
+ * SVS_ERR_INVALID_ARG. With three scales the largest cubes that fit are 56^3 with FP32 storage
+ * (55^3 with the median post-filter), 64^3 with F16/BF16_FLOW32 (63^3 with the median) and
+ * 66^3 with F16/BF16 (64^3 with the median). Calls no cudaMalloc or cudaFree; the descriptors
+ * and tile lists travel to the device as kernel parameters. The first call on a device (and the
+ * first after its context was reset) looks up the array's device address
  * (cudaGetSymbolAddress): make it before any stream capture. Every call reuses the same array
  * and clears the state it uses, so calls that overlap on the GPU (different streams or devices
  * sharing nothing else) race and must be serialized by the caller; the p output and the

@@ -15,9 +15,13 @@
 # no-op unless CUDA_ERROR_CHECK is defined, svs/src/cudaDebug.cuh:15-27), so their outputs stay
 # zero and the stock solver returns u = 0 everywhere. -maxrregcount=80 (a build flag, the same
 # source and arithmetic) lets every kernel launch. Set REF_MAXRREG= (empty) to build stock.
+#
+# Where the reference lives: REF_SRC (its svs/src folder), else SVS_REFERENCE_ROOT/svs/src, else a
+# checkout named `reference` beside this repository (../reference/svs/src from the repo root).
 set -euo pipefail
-REF_SRC=${REF_SRC:-/root/reference/svs/src}
 HERE=$(cd "$(dirname "$0")" && pwd)
+REF_ROOT=${SVS_REFERENCE_ROOT:-$(cd "$HERE/../.." && pwd)/reference}
+REF_SRC=${REF_SRC:-$REF_ROOT/svs/src}
 OUT="$HERE/_ref/opticalFlow_cuda_ext"
 if [ ! -d "$REF_SRC" ]; then
   echo "reference sources not found at $REF_SRC; nothing to build" >&2

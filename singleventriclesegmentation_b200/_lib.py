@@ -17,6 +17,7 @@ c_int, c_float, c_double, c_void_p, c_int64, c_size_t = (
     ctypes.c_int, ctypes.c_float, ctypes.c_double, ctypes.c_void_p, ctypes.c_int64, ctypes.c_size_t)
 
 SVS_OK = 0
+SVS_ERR_TIMEOUT = 4
 STATUS_NAMES = {0: "SVS_OK", 1: "SVS_ERR_INVALID_ARG", 2: "SVS_ERR_OUT_OF_MEMORY",
                 3: "SVS_ERR_LAUNCH", 4: "SVS_ERR_TIMEOUT", 5: "SVS_ERR_UNSUPPORTED",
                 6: "SVS_ERR_CUDA"}
@@ -96,6 +97,7 @@ _SIGS = {
     "svs_tvl1_plan_level_ctas": (c_int64, [c_void_p, c_int]),
     "svs_tvl1_chunk_plan": (c_int, [c_int64, c_int, c_int64, c_void_p, c_void_p, c_void_p]),
     "svs_tvl1_plan_check": (c_int, [c_void_p]),
+    "svs_tvl1_plan_set_stall_test": (c_int, [c_void_p, c_int, c_int, c_int, ctypes.c_uint32]),
     "svs_tvl1_solve_noalloc": (c_int, [ctypes.POINTER(TVL1Params), c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
 }
 

@@ -116,10 +116,12 @@ __device__ __forceinline__ void dual_row(const T D[6], T ex, T ey, T ez, T& p0, 
 
 // Step length along g of the L1 shrinkage, the three cases of opticalFlowOps.cu:140-171 (no
 // divergence): rho < -th: +factor; rho > th: -factor; |rho| <= th: -rho/|g|^2 (0 where
-// |g|^2 <= 1e-10, the reference's (double)g2 > 1e-10 for a float g2).
+// |g|^2 <= 1e-10, the reference's (double)g2 > 1e-10 for a float g2). The division is IEEE
+// round-to-nearest like the reference's; the reference divides each component's product,
+// (-rho g_c)/|g|^2, where this step divides once and the caller multiplies by g_c.
 __device__ __forceinline__ float shrink_step(float rho, float g2s, float factor) {
   const float th = __fmul_rn(factor, g2s);
-  return (rho < -th) ? factor : (rho > th) ? -factor : (g2s >= 1e-10f ? __fdividef(-rho, g2s) : 0.f);
+  return (rho < -th) ? factor : (rho > th) ? -factor : (g2s >= 1e-10f ? __fdiv_rn(-rho, g2s) : 0.f);
 }
 __device__ __forceinline__ float2 shrink_step(float2 rho, float2 g2s, float factor) {
   return make_float2(shrink_step(rho.x, g2s.x, factor), shrink_step(rho.y, g2s.y, factor));
@@ -350,13 +352,13 @@ __device__ __forceinline__ uint64_t global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Bounded wait: gives up after kMbarWaitNs of wall time (a tile's loads complete in microseconds).
-constexpr uint64_t kMbarWaitNs = 2000000000ull;
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait: gives up after limit_ns of wall time (IterArgs::wait_us, 2 s by default; a
+// tile's loads complete in microseconds).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   while (!mbar_try_wait(bar, parity))
-    if (global_ns() - t0 > kMbarWaitNs) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   return true;
 }
 // Plain arrival (release, CTA scope) of this thread on an mbarrier.
@@ -365,12 +367,13 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 }
 // Bounded wait that also gives up as soon as another thread of the CTA has raised `abort`; a
 // thread that times out raises it.
-__device__ __forceinline__ bool mbar_wait_abort(uint64_t* bar, uint32_t parity, volatile int* abort) {
+__device__ __forceinline__ bool mbar_wait_abort(uint64_t* bar, uint32_t parity, volatile int* abort,
+                                                uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_ns();
   while (!mbar_try_wait(bar, parity)) {
     if (*abort) return false;
-    if (global_ns() - t0 > kMbarWaitNs) {
+    if (global_ns() - t0 > limit_ns) {
       *abort = 1;
       return false;
     }
@@ -475,8 +478,11 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
 
   const int kb = max(z0 - 1, 0), ke = min(z1, nz - 1);
   const int pl = max(kb - 1, 0), ph = min(ke + 1, nz - 1);  // planes staged by this tile
+  const uint64_t wait_ns = (uint64_t)a.wait_us * 1000ull;
+  const int stall_r = (int)blockIdx.x == a.stall_cta ? a.stall_plane : -1;
   auto issue = [&](int q) {
     const int r = q - pl;
+    if (r == stall_r) return;  // timeout-path test: this plane's copies are never issued
     uint64_t* bar = bars + r % G::NB;
     unsigned char* U = smem + G::U_OFF + (r % G::NU) * G::U_SLOT;
     if (q < kb) {
@@ -523,7 +529,7 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
     while (waited < need && !bad) {
       ++waited;
       const int r = waited - pl;
-      if (!mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1))) bad = true;
+      if (!mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1), wait_ns)) bad = true;
     }
     const int qs = k % 3;
     // own column of u: planes k-1 and k from the previous step, k+1 read once here
@@ -612,7 +618,7 @@ iterate_tma_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ desc
       // wait (bounded) for the copies this CTA still has in flight before it exits
       for (int q = max(waited + 1, pl); q <= issued; ++q) {
         const int r = q - pl;
-        mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1));
+        mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1), wait_ns);
       }
     }
     return;
@@ -716,10 +722,10 @@ struct SplitGeom {
   static constexpr int NT_LAUNCH = NT + (AS ? 32 : 0);
 };
 
-template <typename SU, typename SP, int TX, int TY, int DIST, int V, int MINB, bool GEN, bool AS = false>
-__global__ void __launch_bounds__(SplitGeom<SU, SP, TX, TY, DIST, V, AS>::NT_LAUNCH, MINB)
-iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs,
-                     const TMaps* __restrict__ maps, IterArgs a, int* __restrict__ status) {
+template <typename SU, typename SP, int TX, int TY, int DIST, int V, bool GEN, bool AS>
+__device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const Desc* __restrict__ descs,
+                                           const TMaps* __restrict__ maps, const IterArgs a,
+                                           int* __restrict__ status) {
   using G = SplitGeom<SU, SP, TX, TY, DIST, V, AS>;
   using B = typename G::B;
   using T = LaneT<V>;
@@ -784,8 +790,11 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
 
   const int kb = max(z0 - 1, 0), ke = min(z1, nz - 1);
   const int pl = max(kb - 1, 0), ph = min(ke + 1, nz - 1);
+  const uint64_t wait_ns = (uint64_t)a.wait_us * 1000ull;
+  const int stall_r = (int)blockIdx.x == a.stall_cta ? a.stall_plane : -1;
   auto issue = [&](int q) {
     const int r = q - pl;
+    if (r == stall_r) return;  // timeout-path test: this plane's copies are never issued
     uint64_t* bar = bars + r % G::NB;
     unsigned char* U = smem + G::U_OFF + (r % G::NU) * B::U_SLOT;
     if (q < kb) {
@@ -834,7 +843,7 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
         issued = last;
         for (int q = kb + DIST; q <= ph; ++q) {
           const int st = q - DIST - kb;
-          if (!mbar_wait_abort(freed + st % G::NFR, (uint32_t)((st / G::NFR) & 1), abort_flag)) break;
+          if (!mbar_wait_abort(freed + st % G::NFR, (uint32_t)((st / G::NFR) & 1), abort_flag, wait_ns)) break;
           issue(q);
           issued = q;
         }
@@ -843,7 +852,7 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
           // wait (bounded) for the copies still in flight before the CTA may exit
           for (int q = max(issued - G::NB + 1, pl); q <= issued; ++q) {
             const int r = q - pl;
-            mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1));
+            mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1), wait_ns);
           }
         }
       }
@@ -911,12 +920,12 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
   // AS: waits on "q rows of plane j published" and "step j done by every lane"
   auto wait_q = [&](int j) {
     const int r = j - kb;
-    return mbar_wait_abort(qpub + (r & 1), (uint32_t)((r >> 1) & 1), abort_flag);
+    return mbar_wait_abort(qpub + (r & 1), (uint32_t)((r >> 1) & 1), abort_flag, wait_ns);
   };
   auto wait_free = [&](int j) {
     if constexpr (AS) {
       const int r = j - kb;
-      return mbar_wait_abort(freed + r % G::NFR, (uint32_t)((r / G::NFR) & 1), abort_flag);
+      return mbar_wait_abort(freed + r % G::NFR, (uint32_t)((r / G::NFR) & 1), abort_flag, wait_ns);
     } else {
       return true;  // only the decoupled form waits here
     }
@@ -929,8 +938,8 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
     while (waited < need && !bad) {
       ++waited;
       const int r = waited - pl;
-      const bool ok = AS ? mbar_wait_abort(bars + r % G::NB, (uint32_t)((r / G::NB) & 1), abort_flag)
-                         : mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1));
+      const bool ok = AS ? mbar_wait_abort(bars + r % G::NB, (uint32_t)((r / G::NB) & 1), abort_flag, wait_ns)
+                         : mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1), wait_ns);
       if (!ok) bad = true;
     }
     if (AS && bad) return;
@@ -1101,7 +1110,7 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
       // wait (bounded) for the copies this CTA still has in flight before it exits
       for (int q = max(waited + 1, pl); q <= issued; ++q) {
         const int r = q - pl;
-        mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1));
+        mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1), wait_ns);
       }
     }
     return;
@@ -1122,17 +1131,41 @@ iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ de
   }
 }
 
+// The split-role kernel with a register budget for MINB resident CTAs per SM (launch bounds)...
+template <typename SU, typename SP, int TX, int TY, int DIST, int V, int MINB, bool GEN, bool AS = false>
+__global__ void __launch_bounds__(SplitGeom<SU, SP, TX, TY, DIST, V, AS>::NT_LAUNCH, MINB)
+iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs,
+                     const TMaps* __restrict__ maps, IterArgs a, int* __restrict__ status) {
+  split_body<SU, SP, TX, TY, DIST, V, GEN, AS>(tiles, descs, maps, a, status);
+}
+// ...or with an explicit per-thread register cap: the launch-bounds arithmetic rounds a block of
+// 5.5 warps up further than the register file requires, so three 176-thread CTAs per SM (6
+// warps x 112 registers x 32 lanes each, 64,512 of the 65,536 registers) need the cap spelled out.
+template <typename SU, typename SP, int TX, int TY, int DIST, int V, int REGS, bool GEN, bool AS = false>
+__global__ void __launch_bounds__(SplitGeom<SU, SP, TX, TY, DIST, V, AS>::NT_LAUNCH) __maxnreg__(REGS)
+iterate_split_kernel_r(const Tile* __restrict__ tiles, const Desc* __restrict__ descs,
+                       const TMaps* __restrict__ maps, IterArgs a, int* __restrict__ status) {
+  split_body<SU, SP, TX, TY, DIST, V, GEN, AS>(tiles, descs, maps, a, status);
+}
+
 // Compiled shapes of the split-role form (tile, prefetch distance, voxels per lane, CTAs per SM
-// the register budget is sized for); instantiated in svs_split.cu.
+// the register budget is sized for, or an explicit register cap); instantiated in svs_split.cu.
 struct SplitShape {
   int tx, ty, dist, v, minb;
-  bool as;  // decoupled synchronisation (mbarriers and a producer warp instead of __syncthreads)
+  bool as;   // decoupled synchronisation (mbarriers and a producer warp instead of __syncthreads)
+  int regs;  // > 0: registers per thread (iterate_split_kernel_r), instead of minb
 };
 constexpr SplitShape kSplitShapes[] = {
-    {32, 8, 3, 2, 1, false},  {32, 8, 4, 2, 1, false},  {16, 16, 3, 2, 1, false}, {40, 8, 3, 2, 2, false},
-    {32, 16, 3, 2, 1, false}, {40, 16, 3, 2, 1, false}, {32, 8, 3, 1, 2, false},  {32, 8, 4, 1, 2, false},
-    {16, 16, 3, 1, 2, false}, {32, 16, 2, 1, 1, false}, {32, 16, 3, 1, 1, false}, {40, 8, 3, 1, 2, false},
-    {40, 8, 3, 2, 2, true},   {32, 8, 3, 2, 2, true},   {16, 16, 3, 1, 2, true},  {32, 16, 3, 2, 1, true}};
+    {32, 8, 3, 2, 1, false, 0},  {32, 8, 4, 2, 1, false, 0},  {16, 16, 3, 2, 1, false, 0},
+    {40, 8, 3, 2, 2, false, 0},  {32, 16, 3, 2, 1, false, 0}, {40, 16, 3, 2, 1, false, 0},
+    {32, 8, 3, 1, 2, false, 0},  {32, 8, 4, 1, 2, false, 0},  {16, 16, 3, 1, 2, false, 0},
+    {32, 16, 2, 1, 1, false, 0}, {32, 16, 3, 1, 1, false, 0}, {40, 8, 3, 1, 2, false, 0},
+    {40, 8, 3, 2, 2, true, 0},   {32, 8, 3, 2, 2, true, 0},   {16, 16, 3, 1, 2, true, 0},
+    {32, 16, 3, 2, 1, true, 0},
+    // three CTAs per SM (5.5 warps each, 72.6 KB / 66.8 KB of shared memory with 16-bit fields)
+    {16, 16, 2, 2, 3, false, 112}, {32, 8, 2, 2, 3, false, 112},
+    // two CTAs per SM with the 16x16 tile (no partial tiles at widths that are multiples of 16)
+    {16, 16, 3, 2, 2, false, 0}};
 constexpr int kNumSplitShapes = sizeof(kSplitShapes) / sizeof(kSplitShapes[0]);
 
 // Split-role variant `idx` for a storage mode. op 0: set the kernels' shared-memory attribute

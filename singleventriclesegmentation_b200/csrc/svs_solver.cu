@@ -52,7 +52,8 @@ constexpr TileShape kTileShapes[] = {
     split_entry(0),        split_entry(1),        split_entry(2),        split_entry(3),
     split_entry(4),        split_entry(5),        split_entry(6),        split_entry(7),
     split_entry(8),        split_entry(9),        split_entry(10),       split_entry(11),
-    split_entry(12),       split_entry(13),       split_entry(14),       split_entry(15)};
+    split_entry(12),       split_entry(13),       split_entry(14),       split_entry(15),
+    split_entry(16),       split_entry(17),       split_entry(18)};
 constexpr bool split_table_complete() {
   int n = 0;
   for (const TileShape& t : kTileShapes) n += t.form == kSplit;
@@ -587,6 +588,9 @@ struct svs_plan {
   float* d_reslog = nullptr;               // [pairs][levels][max_warps]
   float** d_snaps = nullptr;               // [pairs] -> [3][n0] floats
   std::vector<float*> snaps;
+  // bounded pipeline waits (svs_tvl1_plan_set_stall_test)
+  unsigned wait_us = 2000000;
+  int stall_level = -1, stall_cta = -1, stall_plane = -1;
 };
 
 namespace svs {
@@ -985,6 +989,9 @@ IterArgs iter_args(const svs_plan& P, int it, int cur) {
   a.wtv = P.prm.weight_tv;
   a.src = cur;
   a.bdry = P.prm.boundary;
+  a.wait_us = P.wait_us;
+  a.stall_cta = -1;
+  a.stall_plane = -1;
   return a;
 }
 
@@ -1003,14 +1010,19 @@ void join_groups(svs_plan& P, int l, cudaStream_t s) {
   }
 }
 // One iteration of level l over all its pairs; returns the launches issued.
-int level_iteration(svs_plan& P, int l, const IterArgs& a, cudaStream_t s) {
+int level_iteration(svs_plan& P, int l, const IterArgs& a_in, cudaStream_t s) {
+  IterArgs a = a_in;
+  if (l == P.stall_level) {
+    a.stall_cta = P.stall_cta;
+    a.stall_plane = P.stall_plane;
+  }
   iter_dispatch(P, nullptr, l, P.level_tile[l], 1, &a, s);
   for (size_t g = 0; g < level_groups(P, l); ++g) {
     const svs_plan::TileGroup& grp = P.extra[l][g];
     P.launch_override = true;
     P.launch_tiles = grp.d;
     P.launch_count = (unsigned)grp.h.size();
-    iter_dispatch(P, nullptr, l, grp.tid, 1, &a, P.side[g]);
+    iter_dispatch(P, nullptr, l, grp.tid, 1, &a_in, P.side[g]);
     P.launch_override = false;
   }
   return 1 + (int)level_groups(P, l);
@@ -1497,7 +1509,22 @@ svs_status svs_tvl1_plan_check(svs_plan* P) {
   int flags = 0;
   svs_status st = check_cuda(cudaMemcpy(&flags, P->d_status, sizeof(int), cudaMemcpyDeviceToHost), "svs_tvl1_plan_check");
   if (st) return st;
+  if (flags) {
+    st = check_cuda(cudaMemset(P->d_status, 0, sizeof(int)), "svs_tvl1_plan_check");  // reported once
+    if (st) return st;
+  }
   if (flags & SVS_DEV_TIMEOUT) return fail(SVS_ERR_TIMEOUT, "a pipeline wait in the iterate kernel timed out; results are invalid");
+  return SVS_OK;
+}
+
+svs_status svs_tvl1_plan_set_stall_test(svs_plan* P, int level, int cta, int plane, uint32_t wait_us) {
+  SVS_REQUIRE(P, "svs_tvl1_plan_set_stall_test: null plan");
+  SVS_REQUIRE(level < P->levels, "svs_tvl1_plan_set_stall_test: bad level");
+  P->stall_level = (level >= 0 && cta >= 0 && plane >= 0) ? level : -1;
+  P->stall_cta = P->stall_level >= 0 ? cta : -1;
+  P->stall_plane = P->stall_level >= 0 ? plane : -1;
+  P->wait_us = wait_us ? wait_us : 2000000u;
+  ++P->tile_epoch;  // the captured graph carries the launch arguments
   return SVS_OK;
 }
 
@@ -1521,24 +1548,66 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 unsigned char* g_noalloc_ptr[kMaxDevices] = {};
+CUcontext g_noalloc_ctx[kMaxDevices] = {};
+
+// The calling thread's current driver context (null if it cannot be read).
+CUcontext current_context() {
+  static PFN_cuCtxGetCurrent_v4000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 4000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(p);
+  }
+  CUcontext c = nullptr;
+  if (fn) fn(&c);
+  return c;
+}
 
 // Device address of the scratch array on the current device: set up once per device (with that
-// device current) through cudaGetSymbolAddress; in host code the array's name is only a host-side
-// stand-in and must never be handed to a kernel.
+// device current) through cudaGetSymbolAddress, and again if the device's context has been
+// replaced since (a reset reloads the module, and the array may move); in host code the array's
+// name is only a host-side stand-in and must never be handed to a kernel.
 svs_status noalloc_scratch(unsigned char** out) {
   int dev = 0;
   svs_status st = check_cuda(cudaGetDevice(&dev), "svs_tvl1_solve_noalloc: cudaGetDevice");
   if (st) return st;
   if (dev < 0 || dev >= kMaxDevices) return fail(SVS_ERR_UNSUPPORTED, "svs_tvl1_solve_noalloc: device index out of range");
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
+  const CUcontext ctx = current_context();
+  if (!g_noalloc_ptr[dev] || ctx != g_noalloc_ctx[dev]) {
     void* p = nullptr;
     st = check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "svs_tvl1_solve_noalloc: cudaGetSymbolAddress");
     if (st) return st;
     g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    g_noalloc_ctx[dev] = current_context();  // the lookup makes the primary context current
   }
   *out = g_noalloc_ptr[dev];
   return SVS_OK;
+}
+
+// The solve's metadata (descriptors, pointer table, tile lists) reaches the scratch as kernel
+// parameters: a launch copies its parameters when it is enqueued, so no host buffer has to
+// outlive the call and no host-to-device copy is queued.
+struct UploadChunk {
+  unsigned char bytes[3840];
+};
+__global__ void upload_kernel(unsigned char* __restrict__ dst, const __grid_constant__ UploadChunk c, unsigned n) {
+  for (unsigned i = threadIdx.x; i < n; i += blockDim.x) dst[i] = c.bytes[i];
+}
+// Returns the number of launches issued (-1 after a launch error).
+long long upload(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  const unsigned char* p = static_cast<const unsigned char*>(src);
+  long long launches = 0;
+  for (size_t off = 0; off < bytes; off += sizeof(UploadChunk::bytes)) {
+    UploadChunk c;
+    const unsigned n = (unsigned)std::min(sizeof(c.bytes), bytes - off);
+    std::memcpy(c.bytes, p + off, n);
+    upload_kernel<<<1, 256, 0, s>>>(static_cast<unsigned char*>(dst) + off, c, n);
+    ++launches;
+  }
+  return cudaPeekAtLastError() == cudaSuccess ? launches : -1;
 }
 
 }  // namespace
@@ -1676,19 +1745,22 @@ extern "C" svs_status svs_tvl1_solve_noalloc(const svs_tvl1_params* prm, const f
     for (size_t i = 0; i < k3.size(); ++i) P.blur.w[i] = k3[i] / tot;
     P.blur_r = ks / 2;
   }
-  // Metadata into the scratch (pageable sources: each copy returns once the data is staged),
-  // then clear the state region so no value from an earlier call is ever read.
+  // Metadata into the scratch (as kernel parameters), then clear the state region so no value
+  // from an earlier call is ever read.
   cudaStream_t s = stream;
-  st = check_cuda(cudaMemcpyAsync(P.d_descs, P.h_descs.data(), P.levels * sizeof(Desc), cudaMemcpyHostToDevice, s), "svs_tvl1_solve_noalloc");
-  if (!st) st = check_cuda(cudaMemcpyAsync(ptrs, hp.data(), hp.size() * sizeof(float*), cudaMemcpyHostToDevice, s), "svs_tvl1_solve_noalloc");
-  for (int l = 0; l < P.levels && !st; ++l)
-    st = check_cuda(cudaMemcpyAsync(P.d_tiles[l], P.h_tiles[l].data(), P.h_tiles[l].size() * sizeof(Tile),
-                                    cudaMemcpyHostToDevice, s), "svs_tvl1_solve_noalloc");
-  if (!st) st = check_cuda(cudaMemsetAsync(state_begin, 0, (size_t)(cur - state_begin), s), "svs_tvl1_solve_noalloc");
+  long long up = upload(P.d_descs, P.h_descs.data(), P.levels * sizeof(Desc), s);
+  const long long up_ptrs = up < 0 ? -1 : upload(ptrs, hp.data(), hp.size() * sizeof(float*), s);
+  up = up_ptrs < 0 ? -1 : up + up_ptrs;
+  for (int l = 0; l < P.levels && up >= 0; ++l) {
+    const long long n = upload(P.d_tiles[l], P.h_tiles[l].data(), P.h_tiles[l].size() * sizeof(Tile), s);
+    up = n < 0 ? -1 : up + n;
+  }
+  if (up < 0) return fail(SVS_ERR_LAUNCH, std::string("svs_tvl1_solve_noalloc: launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+  st = check_cuda(cudaMemsetAsync(state_begin, 0, (size_t)(cur - state_begin), s), "svs_tvl1_solve_noalloc");
   if (st) return st;
   P.warm = false;
   const long long nl = enqueue(P, s);
   if (nl < 0) return fail(SVS_ERR_LAUNCH, std::string("svs_tvl1_solve_noalloc: launch failed: ") + cudaGetErrorString(cudaGetLastError()));
-  count_launches((uint64_t)nl);
+  count_launches((uint64_t)(nl + up));
   return SVS_OK;
 }

@@ -11,8 +11,15 @@ bool run(int op, bool gen, unsigned nt, const Tile* tiles, const Desc* descs, co
          const IterArgs* a, int* status, cudaStream_t s, int* box) {
   constexpr SplitShape S = kSplitShapes[I];
   using G = SplitGeom<SU, SP, S.tx, S.ty, S.dist, S.v, S.as>;
-  auto* kf = iterate_split_kernel<SU, SP, S.tx, S.ty, S.dist, S.v, S.minb, false, S.as>;
-  auto* kt = iterate_split_kernel<SU, SP, S.tx, S.ty, S.dist, S.v, S.minb, true, S.as>;
+  using KFn = void (*)(const Tile*, const Desc*, const TMaps*, IterArgs, int*);
+  KFn kf, kt;
+  if constexpr (S.regs > 0) {
+    kf = iterate_split_kernel_r<SU, SP, S.tx, S.ty, S.dist, S.v, S.regs, false, S.as>;
+    kt = iterate_split_kernel_r<SU, SP, S.tx, S.ty, S.dist, S.v, S.regs, true, S.as>;
+  } else {
+    kf = iterate_split_kernel<SU, SP, S.tx, S.ty, S.dist, S.v, S.minb, false, S.as>;
+    kt = iterate_split_kernel<SU, SP, S.tx, S.ty, S.dist, S.v, S.minb, true, S.as>;
+  }
   if (op == 2) {  // resident CTAs per SM (after op 0 set the shared-memory attribute)
     if (G::SMEM > 227 * 1024) return false;
     int n = 0;
@@ -45,11 +52,12 @@ bool dispatch(int idx, int op, bool gen, unsigned nt, const Tile* tiles, const D
               const IterArgs* a, int* status, cudaStream_t s, int* box) {
 #define SVS_SPLIT(I) \
   case I: return run<SU, SP, I>(op, gen, nt, tiles, descs, maps, a, status, s, box);
-  static_assert(kNumSplitShapes == 16, "one case per compiled shape");
+  static_assert(kNumSplitShapes == 19, "one case per compiled shape");
   switch (idx) {
     SVS_SPLIT(0) SVS_SPLIT(1) SVS_SPLIT(2) SVS_SPLIT(3) SVS_SPLIT(4) SVS_SPLIT(5)
     SVS_SPLIT(6) SVS_SPLIT(7) SVS_SPLIT(8) SVS_SPLIT(9) SVS_SPLIT(10) SVS_SPLIT(11)
-    SVS_SPLIT(12) SVS_SPLIT(13) SVS_SPLIT(14) SVS_SPLIT(15)
+    SVS_SPLIT(12) SVS_SPLIT(13) SVS_SPLIT(14) SVS_SPLIT(15) SVS_SPLIT(16) SVS_SPLIT(17)
+    SVS_SPLIT(18)
     default: return false;
   }
 #undef SVS_SPLIT

@@ -92,6 +92,11 @@ struct Tile {
 struct IterArgs {
   float sigma, tau, factor, wtv;
   int src, bdry;
+  // bounded pipeline waits give up after wait_us microseconds; the CTA with blockIdx.x ==
+  // stall_cta leaves the copies of its staged plane number stall_plane (counted from its first
+  // staged plane) unissued (a test of the timeout path; stall_cta < 0: off)
+  unsigned wait_us;
+  int stall_cta, stall_plane;
 };
 
 // TMA descriptors of one (pair, level): the two ping-pong copies of u and p, D, rc and gw.

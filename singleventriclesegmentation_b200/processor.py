@@ -10,7 +10,8 @@ one batch; the median filter runs on the device inside the solve.
 from __future__ import annotations
 
 import os
-from typing import List, Tuple
+from concurrent.futures import Future, ThreadPoolExecutor
+from typing import List, Sequence, Tuple
 
 import numpy as np
 import torch
@@ -58,6 +59,67 @@ def save_flow(out_dir: str, name: str, mode: str, us: torch.Tensor) -> str:
     path = flow_path(out_dir, name, mode)
     np.save(path, us.detach().float().cpu().numpy())
     return path
+
+
+class FlowWriter:
+    """Asynchronous flow-file output. A submitted flow array is copied device -> pinned host on a
+    copy stream of its own (after an event that marks the end of the solve that produced it) and
+    written as `{name}_{mode}_flow.npy` by a writer thread, so that the next patient's solve on the
+    compute stream overlaps both the copy and the file write. Files are the bytes save_flow
+    writes (processor.py:120)."""
+
+    def __init__(self, device=None):
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.stream = torch.cuda.Stream(self.device)
+        self.pool = ThreadPoolExecutor(max_workers=1)
+        self.futures: List[Future] = []
+
+    def submit(self, out_dir: str, name: str, mode: str, us: torch.Tensor) -> Future:
+        """Queue `us` ([T-1, 3, X, Y, Z] float32 on the device, produced on the current stream)."""
+        src = us.detach().float()
+        solved = torch.cuda.Event()
+        solved.record(torch.cuda.current_stream(self.device))
+        host = torch.empty(src.shape, dtype=torch.float32, pin_memory=True)
+        copied = torch.cuda.Event()
+        with torch.cuda.stream(self.stream):
+            self.stream.wait_event(solved)
+            host.copy_(src, non_blocking=True)
+            copied.record(self.stream)
+        src.record_stream(self.stream)  # the device buffer stays allocated until the copy is done
+        os.makedirs(out_dir, exist_ok=True)
+        path = flow_path(out_dir, name, mode)
+
+        def write() -> str:
+            copied.synchronize()
+            np.save(path, host.numpy())
+            return path
+
+        fut = self.pool.submit(write)
+        self.futures.append(fut)
+        return fut
+
+    def close(self) -> List[str]:
+        """Wait for every queued file; returns their paths in submission order."""
+        paths = [f.result() for f in self.futures]
+        self.futures.clear()
+        self.pool.shutdown(wait=True)
+        return paths
+
+
+def process_patients(patients: Sequence[Tuple[str, torch.Tensor, int, int]], solver, out_dir: str,
+                     modes: Sequence[str] = ("forward", "backward"), median_kernel: int = 3) -> List[str]:
+    """The processor's patient loop (processor.py:95-121 per patient and direction) with the flow
+    files written asynchronously: patients are (name, img [T,Z,Y,X] on the device, tdia, tsys);
+    each patient's pairs run as one batched solve, and its flows go to disk through a FlowWriter
+    while the next one is solved. Returns the written paths."""
+    writer = FlowWriter(solver.device)
+    try:
+        for name, img, tdia, tsys in patients:
+            for mode in modes:
+                writer.submit(out_dir, name, mode, process_sequence(img, tdia, tsys, mode, solver, median_kernel))
+    finally:
+        paths = writer.close()
+    return paths
 
 
 def load_flow(out_dir: str, name: str, mode: str) -> np.ndarray:

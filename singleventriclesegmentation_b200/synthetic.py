@@ -118,13 +118,16 @@ def frame_pair(shape=(80, 80, 80), seed: int = 0, amplitude: float = 2.0, noise:
 
 
 def cine_sequence(T: int = 35, shape=(80, 80, 80), seed: int = 0, amplitude: float = 1.0,
-                  max_disp: float = 3.0, noise: float = 0.01, device: str = "cpu") -> np.ndarray:
-    """[T,Z,Y,X] float32: frame t = I0 warped by amplitude sin(2 pi t / T) v(x), plus noise."""
+                  max_disp: float = 3.0, noise: float = 0.01, device: str = "cpu",
+                  first: int = None) -> np.ndarray:
+    """[T,Z,Y,X] float32: frame t = I0 warped by amplitude sin(2 pi t / T) v(x), plus noise.
+    With `first`, only frames 0 .. first-1 are made (bitwise those of the whole sequence)."""
     rng = np.random.default_rng(seed)
     I0 = blobs_volume(shape, rng)
     v = smooth_field(shape, rng, max_disp)
-    frames = np.empty((T,) + tuple(shape), dtype=np.float32)
-    for t in range(T):
+    n = T if first is None else min(T, first)
+    frames = np.empty((n,) + tuple(shape), dtype=np.float32)
+    for t in range(n):
         a = amplitude * math.sin(2 * math.pi * t / T)
         f = I0 if a == 0.0 else warp_volume(I0, a * v, device)
         frames[t] = (f + rng.normal(0.0, noise, size=tuple(shape))).astype(np.float32)

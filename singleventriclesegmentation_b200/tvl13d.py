@@ -73,6 +73,12 @@ class SolverPlan:
         with torch.cuda.device(self.device):
             check(_lib.lib().svs_tvl1_plan_check(self._h))
 
+    def set_stall_test(self, level: int = -1, cta: int = -1, plane: int = -1, wait_us: int = 0) -> None:
+        """Test hook of the bounded pipeline waits: at `level`, CTA `cta` never issues the copies
+        of its staged plane number `plane`, and waits give up after wait_us (0 = 2 s); the next
+        check() then raises with SVS_ERR_TIMEOUT. No arguments switch the stall off."""
+        check(_lib.lib().svs_tvl1_plan_set_stall_test(self._h, int(level), int(cta), int(plane), int(wait_us)))
+
     def level_tiles(self):
         return [int(_lib.lib().svs_tvl1_plan_level_tile(self._h, l)) for l in range(8)]
 

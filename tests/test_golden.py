@@ -9,6 +9,9 @@ import pytest
 import torch
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+# bounds on the 32^3 default-configuration solve against the reference's flow (voxels, mean and
+# 99th percentile of the end-point error): about 3x the spread measured on a B200
+SOLVE32_MEAN_TOL, SOLVE32_P99_TOL = 0.005, 0.05
 INTERP = ["NEAREST", "LINEAR", "CUBIC_HERMITESPLINE"]
 BDRY = ["NEAREST", "MIRROR", "REFLECT"]
 
@@ -82,8 +85,9 @@ def test_oracle_solver_matches_reference_solver(oracle):
     u, _ = oracle.tvl1_compute(d["I0"], d["I1"], oracle.SolverParams(), dtype=np.float32)
     for key in ("u", "u_notf32"):
         e = epe(u, d[key])
-        assert e.mean() <= 0.05, (key, e.mean())
-        assert np.percentile(e, 99) <= 0.25, (key, np.percentile(e, 99))
+        print("oracle", key, "mean EPE", e.mean(), "p99", np.percentile(e, 99), "max", e.max())
+        assert e.mean() <= SOLVE32_MEAN_TOL, (key, e.mean())
+        assert np.percentile(e, 99) <= SOLVE32_P99_TOL, (key, np.percentile(e, 99))
 
 
 def test_oracle_masks_match_reference(oracle):
@@ -159,8 +163,8 @@ def test_fused_solver_matches_reference_solver(cuda, oracle):
     for key in ("u", "u_notf32"):
         e = epe(u.cpu().numpy(), d[key])
         print(key, "mean EPE", e.mean(), "p99", np.percentile(e, 99), "max", e.max())
-        assert e.mean() <= 0.05, (key, e.mean())
-        assert np.percentile(e, 99) <= 0.25
+        assert e.mean() <= SOLVE32_MEAN_TOL, (key, e.mean())
+        assert np.percentile(e, 99) <= SOLVE32_P99_TOL
 
 
 @pytest.mark.gpu
@@ -173,3 +177,28 @@ def test_masks_match_reference(cuda):
     for t in range(fwd.shape[0]):
         assert dice(fwd[t, 0], T(d["fwd"][t, 0])) >= 0.99
         assert dice(bwd[t, 0], T(d["bwd"][t, 0])) >= 0.99
+
+
+@pytest.mark.gpu
+def test_reference_call_sequence_on_this_module(cuda, oracle):
+    """Drop-in check: the reference's own per-operator call sequence (tvl13d.py:69-255 and
+    warping.py:49-65, 205-243, restated operator call by operator call in oracle/ref_driver.py)
+    run against this repository's `opticalFlow_cuda_ext.opticalFlow` import shim, which is what
+    the reference's unchanged Python would call. The flow meets the fused solver's bounds against
+    the reference's own 32^3 solve; the mask chain, driven through WarpingCNN3D with the
+    reference's flows, reproduces the reference's chain."""
+    from oracle import ref_driver
+    from opticalFlow_cuda_ext import opticalFlow as of
+    d = load("ref_solve32.npz")
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device="cuda")
+    u, _ = ref_driver.tvl1_compute(of, T(d["I0"]), T(d["I1"]), oracle.SolverParams())
+    for key in ("u", "u_notf32"):
+        e = epe(u.cpu().numpy(), d[key])
+        print("drop-in", key, "mean EPE", e.mean(), "p99", np.percentile(e, 99))
+        assert e.mean() <= SOLVE32_MEAN_TOL and np.percentile(e, 99) <= SOLVE32_P99_TOL
+    m = load("ref_masks.npz")
+    fm, bm = ref_driver.propagate_masks(of, T(m["m0"])[None, None], T(m["mT"])[None, None], T(m["ff"]), T(m["bf"]))
+    fm, bm = fm.cpu().numpy()[:, 0], bm.cpu().numpy()[:, 0]
+    for t in range(fm.shape[0]):
+        assert oracle.dice(fm[t], m["fwd"][t, 0]) >= 0.999
+        assert oracle.dice(bm[t], m["bwd"][t, 0]) >= 0.999
