@@ -404,12 +404,14 @@ __device__ __forceinline__ int gy_of(const Tile& T, int tid, int px) { return T.
 // Plane k+DIST is issued after the barrier of step k, into the u/rc-gw slot of plane k-2 and the
 // p/D slot of plane k, all of which every thread has finished reading by then. The first plane
 // (k = kb-1, the z-neighbour of the first dual plane) carries u only.
-template <typename SU, typename SP, int TX, int TY, int DIST>
+template <typename SU, typename SP, int TX, int TY, int DIST, int UPAD = 0>
 struct TmaGeom {
   static constexpr int ESU = (int)sizeof(SU), ESP = (int)sizeof(SP);
   static constexpr int AU = 16 / ESU, AP = 16 / ESP;      // 16-byte alignment in elements
   static constexpr int PX = TX + 2, PY = TY + 2;
-  static constexpr int UXB = round_up_c(TX + AU + 2, AU);  // u box: x in [x0-AU, x0-AU+UXB)
+  // u box: x in [x0-AU, x0-AU+UXB); UPAD extra columns (a multiple of AU) only widen the row
+  // pitch in shared memory (a bank-conflict choice), the copy reads them as well
+  static constexpr int UXB = round_up_c(TX + AU + 2, AU) + UPAD;
   static constexpr int PXB = round_up_c(TX + AP + 1, AP);  // p/D box: x in [x0-AP, x0-AP+PXB)
   static constexpr int UYB = TY + 4, PYB = TY + 2;         // u rows from y0-2, p/D from y0-1
   static constexpr int U_TX = 3 * UYB * UXB * ESU;
@@ -693,9 +695,10 @@ __device__ __forceinline__ float next_x(float, float R) { return R; }
 __device__ __forceinline__ float2 prev_x(float L, float2 o) { return make_float2(L, o.x); }
 __device__ __forceinline__ float2 next_x(float2 o, float R) { return make_float2(o.y, R); }
 
-template <typename SU, typename SP, int TX, int TY, int DIST, int V, bool AS = false>
+template <typename SU, typename SP, int TX, int TY, int DIST, int V, bool AS = false, int UPAD = 0>
 struct SplitGeom {
-  using B = TmaGeom<SU, SP, TX, TY, DIST>;  // box shapes (shared with the tensor maps)
+  using B = TmaGeom<SU, SP, TX, TY, DIST, UPAD>;  // box shapes (shared with the tensor maps)
+  static_assert(UPAD % B::AU == 0, "padding keeps the 16-byte row alignment");
   static_assert(V == 1 || V == 2, "one or two voxels per lane");
   static_assert(TX % V == 0, "whole lanes per row");
   static constexpr int PW = TX / V;          // lanes per row
@@ -722,11 +725,37 @@ struct SplitGeom {
   static constexpr int NT_LAUNCH = NT + (AS ? 32 : 0);
 };
 
-template <typename SU, typename SP, int TX, int TY, int DIST, int V, bool GEN, bool AS>
+// OPT (schedule options of the interior lanes, the same arithmetic either way):
+//   kLatePrimal  load the primal inputs of plane k-1 (q rows, u, rc, gw) and compute the
+//                shrinkage step AFTER the dual of plane k instead of before it (fewer values live
+//                across the dual, a longer dependent chain per plane);
+//   kJitDual     load the dual field of one flow component at a time and finish that component
+//                (dual, q, p store) before loading the next (fewer values live at once);
+//   kRowPairs    place the interior lanes so that a warp holds 16 voxel pairs of each of two rows
+//                D apart (RowPairs) instead of consecutive lanes along the rows: every 8-byte
+//                shared access of a half-warp is then one row, and the two rows' 4-byte accesses
+//                to 16-bit fields fall in disjoint banks;
+//   OPT >> 8     extra columns of the u box in shared memory (row pitch, TmaGeom::UPAD).
+enum { kLatePrimal = 1, kJitDual = 2, kRowPairs = 4 };
+template <typename SP, int PXB, int PW, int TY, int V>
+struct RowPairs {
+  static constexpr int ROWB = PXB * (int)sizeof(SP);  // bytes per p/D row in shared memory
+  static constexpr int pick() {
+    if (sizeof(SP) == 4) return 1;  // 8-byte accesses: any row distance is conflict-free
+    for (int d = 1; d <= 8; d *= 2)
+      if (TY % (2 * d) == 0 && (d * ROWB) % 128 == 64) return d;
+    return 0;
+  }
+  static constexpr int D = pick();
+  static constexpr bool ok = V == 2 && PW >= 16 && D > 0 && TY % (2 * (D > 0 ? D : 1)) == 0 &&
+                             ((PW - 16) * TY) % 32 == 0;
+  static constexpr int NPAIRED = 16 * TY;  // lanes placed in row pairs; the rest row by row
+};
+template <typename SU, typename SP, int TX, int TY, int DIST, int V, bool GEN, bool AS, int OPT = 0>
 __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const Desc* __restrict__ descs,
                                            const TMaps* __restrict__ maps, const IterArgs a,
                                            int* __restrict__ status) {
-  using G = SplitGeom<SU, SP, TX, TY, DIST, V, AS>;
+  using G = SplitGeom<SU, SP, TX, TY, DIST, V, AS, (OPT >> 8)>;
   using B = typename G::B;
   using T = LaneT<V>;
   constexpr int AU = B::AU, AP = B::AP, UXB = B::UXB, PXB = B::PXB;
@@ -752,8 +781,22 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
   int role, lx, ly;  // position relative to (x0, y0)
   if (tid < G::NI) {
     role = 0;
-    lx = V * (tid % G::PW);
-    ly = tid / G::PW;
+    if constexpr ((OPT & kRowPairs) && RowPairs<SP, PXB, G::PW, TY, V>::ok) {
+      using RP = RowPairs<SP, PXB, G::PW, TY, V>;
+      if (tid < RP::NPAIRED) {
+        const int w = tid >> 5, l = tid & 31, b = w / RP::D;  // warp w: rows r and r + D
+        const int r = b * 2 * RP::D + (w % RP::D) + ((l >> 4) ? RP::D : 0);
+        lx = V * (l & 15);
+        ly = r;
+      } else {  // pairs 16.. of every row, row by row
+        const int i = tid - RP::NPAIRED;
+        lx = V * (16 + i % (G::PW - 16));
+        ly = i / (G::PW - 16);
+      }
+    } else {
+      lx = V * (tid % G::PW);
+      ly = tid / G::PW;
+    }
   } else if (tid < G::NI + G::NH) {
     const int h = tid - G::NI;
     role = 1;
@@ -956,7 +999,8 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
       // primal of plane k-1 with the dual of plane k; lanes outside the volume compute on the
       // zero fill of the boxes (finite values) and store nothing to global memory
       T dxy[3], uo1[3], gp[3], tp;
-      if constexpr (WP) {
+      constexpr bool kEarly = !(OPT & kLatePrimal);
+      if constexpr (WP && kEarly) {
         if (AS && !wait_q(k - 1)) {
           bad = true;
           return;
@@ -967,35 +1011,53 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
       const StencilV<T> fz = bcast_st<T>(fz1);
       const SP* P = reinterpret_cast<const SP*>(PD) + po;
       const SP* Dm = reinterpret_cast<const SP*>(PD + B::P_SLOT) + po;
-      T pk[9], Dk[6], qxo[3], qyo[3];
-#pragma unroll
-      for (int c = 0; c < 9; ++c) pk[c] = Lane<V, SP>::ld(P + c * PC);
+      T Dk[6], qxo[3], qyo[3];
 #pragma unroll
       for (int c = 0; c < 6; ++c) Dk[c] = Lane<V, SP>::ld(Dm + c * PC);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
+      const bool p_out = active && !bad && k >= z0 && k < z1;
+      SP* pdst = p_dst + (long long)k * plane;
+      // the dual of flow component c: p_new, its q = D p_new, and the p store
+      auto dual_comp = [&](int c, T& p0, T& p1, T& p2) {
         const SU* u = Uk + c * UC;
         const T o = Lane<V, SU>::ld(u);
         const T ex = apply3<GEN>(fx, prev_x(Store<SU>::sh(u - 1), o), o, next_x(o, Store<SU>::sh(u + V)));
         const T ey = apply3<GEN>(fy, Lane<V, SU>::ld(u - UXB), o, Lane<V, SU>::ld(u + UXB));
         const T ez = apply3<GEN>(fz, Lane<V, SU>::ld(Um + c * UC), o, Lane<V, SU>::ld(Up + c * UC));
-        dual_row(Dk, ex, ey, ez, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2], a.sigma, a.wtv, wtv2);
-      }
+        dual_row(Dk, ex, ey, ez, p0, p1, p2, a.sigma, a.wtv, wtv2);
+      };
+      auto q_comp = [&](int c, const T& p0, const T& p1, const T& p2) {
+        qyo[c] = dot3(Dk[1], Dk[3], Dk[4], p0, p1, p2);
+        qxo[c] = dot3(Dk[0], Dk[1], Dk[2], p0, p1, p2);
+        qc[c] = dot3(Dk[2], Dk[4], Dk[5], p0, p1, p2);
+      };
+      auto store_p = [&](int c, const T& p) {
+        if (full) Lane<V, SP>::st(pdst + c * cs, p);
+        else Store<SP>::st(pdst + c * cs, first(p));
+      };
+      if constexpr (OPT & kJitDual) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const T* pc = &pk[3 * c];
-        qyo[c] = dot3(Dk[1], Dk[3], Dk[4], pc[0], pc[1], pc[2]);
-        qxo[c] = dot3(Dk[0], Dk[1], Dk[2], pc[0], pc[1], pc[2]);
-        qc[c] = dot3(Dk[2], Dk[4], Dk[5], pc[0], pc[1], pc[2]);
-      }
-      if (active && !bad && k >= z0 && k < z1) {
-        SP* dst = p_dst + (long long)k * plane;
-        if (full) {
+        for (int c = 0; c < 3; ++c) {
+          T p0 = Lane<V, SP>::ld(P + (3 * c) * PC), p1 = Lane<V, SP>::ld(P + (3 * c + 1) * PC),
+            p2 = Lane<V, SP>::ld(P + (3 * c + 2) * PC);
+          dual_comp(c, p0, p1, p2);
+          q_comp(c, p0, p1, p2);
+          if (p_out) {
+            store_p(3 * c, p0);
+            store_p(3 * c + 1, p1);
+            store_p(3 * c + 2, p2);
+          }
+        }
+      } else {
+        T pk[9];
 #pragma unroll
-          for (int c = 0; c < 9; ++c) Lane<V, SP>::st(dst + c * cs, pk[c]);
-        } else {
+        for (int c = 0; c < 9; ++c) pk[c] = Lane<V, SP>::ld(P + c * PC);
 #pragma unroll
-          for (int c = 0; c < 9; ++c) Store<SP>::st(dst + c * cs, first(pk[c]));
+        for (int c = 0; c < 3; ++c) dual_comp(c, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) q_comp(c, pk[3 * c], pk[3 * c + 1], pk[3 * c + 2]);
+        if (p_out) {
+#pragma unroll
+          for (int c = 0; c < 9; ++c) store_p(c, pk[c]);
         }
       }
       // AS: the q slot of plane k was last read by the primal of plane k-2 (step k-1)
@@ -1012,6 +1074,14 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
       }
       if constexpr (AS) mbar_arrive(qpub + ((k - kb) & 1));
       if constexpr (WP) {
+        if constexpr (!kEarly) {
+          if (AS && !wait_q(k - 1)) {
+            bad = true;
+            return;
+          }
+          load_dxy(k - 1, dxy);
+          primal_pre(k - 1, uo1, gp, tp);
+        }
         if (active && !bad) finish_primal(k - 1, dxy, qc, uo1, gp, tp);
       }
     } else {
@@ -1132,40 +1202,56 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
 }
 
 // The split-role kernel with a register budget for MINB resident CTAs per SM (launch bounds)...
-template <typename SU, typename SP, int TX, int TY, int DIST, int V, int MINB, bool GEN, bool AS = false>
+template <typename SU, typename SP, int TX, int TY, int DIST, int V, int MINB, bool GEN, bool AS = false, int OPT = 0>
 __global__ void __launch_bounds__(SplitGeom<SU, SP, TX, TY, DIST, V, AS>::NT_LAUNCH, MINB)
 iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs,
                      const TMaps* __restrict__ maps, IterArgs a, int* __restrict__ status) {
-  split_body<SU, SP, TX, TY, DIST, V, GEN, AS>(tiles, descs, maps, a, status);
+  split_body<SU, SP, TX, TY, DIST, V, GEN, AS, OPT>(tiles, descs, maps, a, status);
 }
 // ...or with an explicit per-thread register cap: the launch-bounds arithmetic rounds a block of
 // 5.5 warps up further than the register file requires, so three 176-thread CTAs per SM (6
 // warps x 112 registers x 32 lanes each, 64,512 of the 65,536 registers) need the cap spelled out.
-template <typename SU, typename SP, int TX, int TY, int DIST, int V, int REGS, bool GEN, bool AS = false>
+template <typename SU, typename SP, int TX, int TY, int DIST, int V, int REGS, bool GEN, bool AS = false, int OPT = 0>
 __global__ void __launch_bounds__(SplitGeom<SU, SP, TX, TY, DIST, V, AS>::NT_LAUNCH) __maxnreg__(REGS)
 iterate_split_kernel_r(const Tile* __restrict__ tiles, const Desc* __restrict__ descs,
                        const TMaps* __restrict__ maps, IterArgs a, int* __restrict__ status) {
-  split_body<SU, SP, TX, TY, DIST, V, GEN, AS>(tiles, descs, maps, a, status);
+  split_body<SU, SP, TX, TY, DIST, V, GEN, AS, OPT>(tiles, descs, maps, a, status);
 }
 
 // Compiled shapes of the split-role form (tile, prefetch distance, voxels per lane, CTAs per SM
-// the register budget is sized for, or an explicit register cap); instantiated in svs_split.cu.
+// the register budget is sized for, or an explicit register cap, schedule options); instantiated
+// in svs_split.cu for the storage modes in `smask` (bit s = SVS_STORAGE s).
 struct SplitShape {
   int tx, ty, dist, v, minb;
-  bool as;   // decoupled synchronisation (mbarriers and a producer warp instead of __syncthreads)
-  int regs;  // > 0: registers per thread (iterate_split_kernel_r), instead of minb
+  bool as;    // decoupled synchronisation (mbarriers and a producer warp instead of __syncthreads)
+  int regs;   // > 0: registers per thread (iterate_split_kernel_r), instead of minb
+  int opt;    // kLatePrimal | kJitDual
+  int smask;  // storage modes compiled
 };
+constexpr int kAllStorages = 31, kF32AndF16Flow32 = (1 << SVS_STORAGE_F32) | (1 << SVS_STORAGE_F16_FLOW32);
 constexpr SplitShape kSplitShapes[] = {
-    {32, 8, 3, 2, 1, false, 0},  {32, 8, 4, 2, 1, false, 0},  {16, 16, 3, 2, 1, false, 0},
-    {40, 8, 3, 2, 2, false, 0},  {32, 16, 3, 2, 1, false, 0}, {40, 16, 3, 2, 1, false, 0},
-    {32, 8, 3, 1, 2, false, 0},  {32, 8, 4, 1, 2, false, 0},  {16, 16, 3, 1, 2, false, 0},
-    {32, 16, 2, 1, 1, false, 0}, {32, 16, 3, 1, 1, false, 0}, {40, 8, 3, 1, 2, false, 0},
-    {40, 8, 3, 2, 2, true, 0},   {32, 8, 3, 2, 2, true, 0},   {16, 16, 3, 1, 2, true, 0},
-    {32, 16, 3, 2, 1, true, 0},
+    {32, 8, 3, 2, 1, false, 0, 0, kAllStorages},  {32, 8, 4, 2, 1, false, 0, 0, kAllStorages},
+    {16, 16, 3, 2, 1, false, 0, 0, kAllStorages}, {40, 8, 3, 2, 2, false, 0, 0, kAllStorages},
+    {32, 16, 3, 2, 1, false, 0, 0, kAllStorages}, {40, 16, 3, 2, 1, false, 0, 0, kAllStorages},
+    {32, 8, 3, 1, 2, false, 0, 0, kAllStorages},  {32, 8, 4, 1, 2, false, 0, 0, kAllStorages},
+    {16, 16, 3, 1, 2, false, 0, 0, kAllStorages}, {32, 16, 2, 1, 1, false, 0, 0, kAllStorages},
+    {32, 16, 3, 1, 1, false, 0, 0, kAllStorages}, {40, 8, 3, 1, 2, false, 0, 0, kAllStorages},
+    {40, 8, 3, 2, 2, true, 0, 0, kAllStorages},   {32, 8, 3, 2, 2, true, 0, 0, kAllStorages},
+    {16, 16, 3, 1, 2, true, 0, 0, kAllStorages},  {32, 16, 3, 2, 1, true, 0, 0, kAllStorages},
     // three CTAs per SM (5.5 warps each, 72.6 KB / 66.8 KB of shared memory with 16-bit fields)
-    {16, 16, 2, 2, 3, false, 112}, {32, 8, 2, 2, 3, false, 112},
+    {16, 16, 2, 2, 3, false, 112, 0, kAllStorages}, {32, 8, 2, 2, 3, false, 112, 0, kAllStorages},
     // two CTAs per SM with the 16x16 tile (no partial tiles at widths that are multiples of 16)
-    {16, 16, 3, 2, 2, false, 0}};
+    {16, 16, 3, 2, 2, false, 0, 0, kAllStorages},
+    // schedule and placement options (FP32 and f16-flow32 storage)
+    {40, 8, 3, 2, 2, false, 0, kJitDual, kF32AndF16Flow32},
+    {40, 8, 3, 2, 2, false, 0, kJitDual | kLatePrimal, kF32AndF16Flow32},
+    {16, 16, 2, 2, 3, false, 112, kJitDual | kLatePrimal, kF32AndF16Flow32},
+    {32, 16, 3, 2, 1, false, 0, kJitDual, kF32AndF16Flow32},
+    {40, 8, 3, 2, 2, false, 0, kRowPairs, kF32AndF16Flow32},
+    {40, 8, 3, 2, 2, false, 0, kRowPairs | (8 << 8), kF32AndF16Flow32},
+    {40, 8, 3, 2, 2, false, 0, kRowPairs | kJitDual, kF32AndF16Flow32},
+    {32, 8, 2, 2, 3, false, 112, kRowPairs | kJitDual | kLatePrimal, kF32AndF16Flow32},
+    {32, 16, 3, 2, 1, false, 0, kRowPairs, kF32AndF16Flow32}};
 constexpr int kNumSplitShapes = sizeof(kSplitShapes) / sizeof(kSplitShapes[0]);
 
 // Split-role variant `idx` for a storage mode. op 0: set the kernels' shared-memory attribute

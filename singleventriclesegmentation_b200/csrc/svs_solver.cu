@@ -53,7 +53,9 @@ constexpr TileShape kTileShapes[] = {
     split_entry(4),        split_entry(5),        split_entry(6),        split_entry(7),
     split_entry(8),        split_entry(9),        split_entry(10),       split_entry(11),
     split_entry(12),       split_entry(13),       split_entry(14),       split_entry(15),
-    split_entry(16),       split_entry(17),       split_entry(18)};
+    split_entry(16),       split_entry(17),       split_entry(18),       split_entry(19),
+    split_entry(20),       split_entry(21),       split_entry(22),       split_entry(23),
+    split_entry(24),       split_entry(25),       split_entry(26),       split_entry(27)};
 constexpr bool split_table_complete() {
   int n = 0;
   for (const TileShape& t : kTileShapes) n += t.form == kSplit;

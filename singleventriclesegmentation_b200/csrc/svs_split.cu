@@ -6,19 +6,30 @@
 namespace svs {
 namespace {
 
+template <typename SU, typename SP> constexpr int storage_id() {
+  if constexpr (std::is_same<SU, float>::value && std::is_same<SP, float>::value) return SVS_STORAGE_F32;
+  else if constexpr (std::is_same<SU, float>::value && std::is_same<SP, __half>::value) return SVS_STORAGE_F16_FLOW32;
+  else if constexpr (std::is_same<SU, float>::value) return SVS_STORAGE_BF16_FLOW32;
+  else if constexpr (std::is_same<SP, __half>::value) return SVS_STORAGE_F16;
+  else return SVS_STORAGE_BF16;
+}
+
 template <typename SU, typename SP, int I>
 bool run(int op, bool gen, unsigned nt, const Tile* tiles, const Desc* descs, const TMaps* maps,
          const IterArgs* a, int* status, cudaStream_t s, int* box) {
   constexpr SplitShape S = kSplitShapes[I];
-  using G = SplitGeom<SU, SP, S.tx, S.ty, S.dist, S.v, S.as>;
+  if constexpr (!(S.smask & (1 << storage_id<SU, SP>()))) {
+    return false;  // not compiled for this storage mode
+  } else {
+  using G = SplitGeom<SU, SP, S.tx, S.ty, S.dist, S.v, S.as, (S.opt >> 8)>;
   using KFn = void (*)(const Tile*, const Desc*, const TMaps*, IterArgs, int*);
   KFn kf, kt;
   if constexpr (S.regs > 0) {
-    kf = iterate_split_kernel_r<SU, SP, S.tx, S.ty, S.dist, S.v, S.regs, false, S.as>;
-    kt = iterate_split_kernel_r<SU, SP, S.tx, S.ty, S.dist, S.v, S.regs, true, S.as>;
+    kf = iterate_split_kernel_r<SU, SP, S.tx, S.ty, S.dist, S.v, S.regs, false, S.as, S.opt>;
+    kt = iterate_split_kernel_r<SU, SP, S.tx, S.ty, S.dist, S.v, S.regs, true, S.as, S.opt>;
   } else {
-    kf = iterate_split_kernel<SU, SP, S.tx, S.ty, S.dist, S.v, S.minb, false, S.as>;
-    kt = iterate_split_kernel<SU, SP, S.tx, S.ty, S.dist, S.v, S.minb, true, S.as>;
+    kf = iterate_split_kernel<SU, SP, S.tx, S.ty, S.dist, S.v, S.minb, false, S.as, S.opt>;
+    kt = iterate_split_kernel<SU, SP, S.tx, S.ty, S.dist, S.v, S.minb, true, S.as, S.opt>;
   }
   if (op == 2) {  // resident CTAs per SM (after op 0 set the shared-memory attribute)
     if (G::SMEM > 227 * 1024) return false;
@@ -45,6 +56,7 @@ bool run(int op, bool gen, unsigned nt, const Tile* tiles, const Desc* descs, co
   }
   (gen ? kt : kf)<<<nt, G::NT_LAUNCH, G::SMEM, s>>>(tiles, descs, maps, *a, status);
   return true;
+  }
 }
 
 template <typename SU, typename SP>
@@ -52,12 +64,13 @@ bool dispatch(int idx, int op, bool gen, unsigned nt, const Tile* tiles, const D
               const IterArgs* a, int* status, cudaStream_t s, int* box) {
 #define SVS_SPLIT(I) \
   case I: return run<SU, SP, I>(op, gen, nt, tiles, descs, maps, a, status, s, box);
-  static_assert(kNumSplitShapes == 19, "one case per compiled shape");
+  static_assert(kNumSplitShapes == 28, "one case per compiled shape");
   switch (idx) {
     SVS_SPLIT(0) SVS_SPLIT(1) SVS_SPLIT(2) SVS_SPLIT(3) SVS_SPLIT(4) SVS_SPLIT(5)
     SVS_SPLIT(6) SVS_SPLIT(7) SVS_SPLIT(8) SVS_SPLIT(9) SVS_SPLIT(10) SVS_SPLIT(11)
     SVS_SPLIT(12) SVS_SPLIT(13) SVS_SPLIT(14) SVS_SPLIT(15) SVS_SPLIT(16) SVS_SPLIT(17)
-    SVS_SPLIT(18)
+    SVS_SPLIT(18) SVS_SPLIT(19) SVS_SPLIT(20) SVS_SPLIT(21) SVS_SPLIT(22) SVS_SPLIT(23)
+    SVS_SPLIT(24) SVS_SPLIT(25) SVS_SPLIT(26) SVS_SPLIT(27)
     default: return false;
   }
 #undef SVS_SPLIT
