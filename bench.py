@@ -11,7 +11,11 @@ flows. The sequence stands in for the reference's 80^3 x 35-frame cine MRI data.
 Before warm-up the iterate-kernel variant of each pyramid level is autotuned on the plan's own
 state. Beside the headline line's contract keys it reports the plain GPU form (the reference's
 per-operator structure on this package's kernels, one 80^3 pair, full schedule) for the ratio the
-metric asks for. Further workloads, one JSON line each, on one GPU:
+metric asks for, `latency` (p50/p99 of the 68-pair sequence from the timed steps, and of one 80^3
+pair solved alone), `fp32_storage` (the same sequence solve with every field stored in FP32) and
+`compute_metrics` (the workload's own end-mask Dice / Hausdorff, warping.py:245-270). The
+reference arm (--impl reference) adds `reference_gpu`: the reference's own CUDA extension on one
+pair of the sequence. Further workloads, one JSON line each, on one GPU:
 
     python bench.py --workload uneven    # 64 pairs, dims per axis on {40, ..., 128}
     python bench.py --workload mixed     # the sequence + 16 x 128^3, 16-bit storage modes, EPE vs FP64 GPU oracle

@@ -7,10 +7,14 @@ chain over the first 12 steps of the 35-frame 80^3 cine sequence (svs/modules/fl
 205-243) with its end metrics (:245-270). The inputs are regenerated here from their seeds and
 checked against the SHA-256 the generator recorded.
 
-Tolerances (measured spread x about 3, stated per test):
-  flow      mean end-point error and its 99th percentile against the reference's flow;
-  masks     per frame Dice >= 0.99 and Hausdorff <= 1 voxel between our chain and the
-            reference's chain; end metrics within 0.01 (Dice) and 1 voxel (Hausdorff).
+Tolerances (about 3x the spread measured on a B200, stated per test):
+  flow      mean end-point error and its 99th percentile against the reference's flow; measured
+            on the single pair: FP32 storage 0.00031 / 0.0021 voxel, f16-flow32 0.00063 / 0.0037
+            (the chain's flows are closer still);
+  masks     per frame Dice >= 0.999 and Hausdorff <= 1 voxel between our chain and the
+            reference's chain (measured: FP32 identical, f16-flow32 worst Dice 0.99992, HD 1);
+            the warped single-pair mask identical up to the same bounds; end metrics within 0.01
+            (Dice) and 1 voxel (Hausdorff) of the reference's (measured: equal).
 """
 import hashlib
 import math
@@ -28,7 +32,7 @@ MASK_T1 = 12
 
 # bounds on the flow against the reference (voxels): mean and 99th percentile of the end-point
 # error, per storage of the iteration state (arithmetic is FP32 in both)
-FLOW_TOL = {"f32": (0.01, 0.05), "f16-flow32": (0.01, 0.05)}
+FLOW_TOL = {"f32": (0.001, 0.0065), "f16-flow32": (0.002, 0.011)}
 
 
 def load(name):
@@ -98,7 +102,7 @@ def test_pair80_flow_and_warped_mask_match_reference(cuda, pair80, storage):
     ref = torch.from_numpy(unbits(d["mask_warped_bits"])).cuda()
     dc, hd = dice(mw, ref), hausdorff(mw, ref)
     print(f"{storage}: warped mask vs reference Dice {dc:.5f} HD {hd}")
-    assert dc >= 0.99 and hd <= 1.0
+    assert dc >= 0.999 and hd <= 1.0
 
 
 @pytest.mark.gpu
@@ -134,7 +138,7 @@ def test_chain80_masks_match_reference(cuda, seq80, storage):
             dc, hd = dice(got, ref), hausdorff(got, ref)
             worst_d, worst_h = min(worst_d, dc), max(worst_h, hd)
     print(f"{storage}: chain vs reference worst Dice {worst_d:.5f} worst HD {worst_h}")
-    assert worst_d >= 0.99 and worst_h <= 1.0
+    assert worst_d >= 0.999 and worst_h <= 1.0
     got = compute_metrics(fm, bm)
     ref = d["compute_metrics"]
     print(f"{storage}: end metrics {got} reference {ref}")
