@@ -218,10 +218,12 @@ svs_status svs_tvl1_plan_destroy(svs_plan* plan);
 size_t svs_tvl1_plan_device_bytes(const svs_plan* plan);
 /* Select the iterate-kernel variant (0 = automatic) for later solves; SVS_ERR_INVALID_ARG for an
  * unknown id. Variants 1-5 are TMA pipelines (tile x prefetch distance: 32x8/2, 32x8/3, 64x4/2,
- * 16x16/2, 32x16/2), 6-8 plain-load forms (32x8, 32x4, 16x16), 9-27 split-role TMA pipelines
+ * 16x16/2, 32x16/2), 6-8 plain-load forms (32x8, 32x4, 16x16), 9-33 split-role TMA pipelines
  * (interior, halo-row and halo-column lanes in separate warps; 21-24 synchronise with mbarriers
- * and a producer warp instead of a block-wide barrier per plane; 25 and 26 are sized for three
- * CTAs per SM; svs_tvl1_tile_info gives each shape). Used by the autotuner. */
+ * and a producer warp instead of a block-wide barrier per plane; 25-33 are placement and
+ * schedule options of the 40x8, 32x16 and 16x16 shapes for FP32 and f16-flow32 storage, other
+ * storages report SVS_ERR_UNSUPPORTED for them; svs_tvl1_tile_info gives each shape). Used by the
+ * autotuner. */
 svs_status svs_tvl1_plan_set_tile(svs_plan* plan, int tile_id);
 /* Same for one pyramid level only (0 = fall back to the plan-wide choice). */
 svs_status svs_tvl1_plan_set_level_tile(svs_plan* plan, int level, int tile_id);

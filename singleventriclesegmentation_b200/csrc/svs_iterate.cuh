@@ -694,6 +694,22 @@ __device__ __forceinline__ float prev_x(float L, float) { return L; }
 __device__ __forceinline__ float next_x(float, float R) { return R; }
 __device__ __forceinline__ float2 prev_x(float L, float2 o) { return make_float2(L, o.x); }
 __device__ __forceinline__ float2 next_x(float2 o, float R) { return make_float2(o.y, R); }
+// x-direction stencil of the lane's voxels, as packed operations on the shifted pairs (prev_x,
+// next_x) or, with SCALAR, as one scalar stencil per voxel written straight into the result's two
+// halves (no shifted pair has to be assembled); bitwise the same per voxel.
+template <bool GEN, bool SCALAR>
+__device__ __forceinline__ float x_stencil(const StencilV<float>& s, float L, float o, float R) {
+  return apply3<GEN>(s, L, o, R);
+}
+template <bool GEN, bool SCALAR>
+__device__ __forceinline__ float2 x_stencil(const StencilV<float2>& s, float L, float2 o, float R) {
+  if constexpr (SCALAR) {
+    return make_float2(apply3<GEN>(Stencil3{s.m.x, s.c.x, s.p.x}, L, o.x, o.y),
+                       apply3<GEN>(Stencil3{s.m.y, s.c.y, s.p.y}, o.x, o.y, R));
+  } else {
+    return apply3<GEN>(s, prev_x(L, o), o, next_x(o, R));
+  }
+}
 
 template <typename SU, typename SP, int TX, int TY, int DIST, int V, bool AS = false, int UPAD = 0>
 struct SplitGeom {
@@ -735,8 +751,12 @@ struct SplitGeom {
 //                D apart (RowPairs) instead of consecutive lanes along the rows: every 8-byte
 //                shared access of a half-warp is then one row, and the two rows' 4-byte accesses
 //                to 16-bit fields fall in disjoint banks;
+//   kScalarX     x-direction stencils of a voxel pair as two scalar stencils (x_stencil);
+//   kNoSel       q rows stored without zeroing lanes outside the volume (their q is zero);
+//   kPeel        planes whose z stencils are the interior ones run a step with those
+//                coefficients fixed and both z-neighbour slots present;
 //   OPT >> 8     extra columns of the u box in shared memory (row pitch, TmaGeom::UPAD).
-enum { kLatePrimal = 1, kJitDual = 2, kRowPairs = 4 };
+enum { kLatePrimal = 1, kJitDual = 2, kRowPairs = 4, kScalarX = 8, kNoSel = 16, kPeel = 32 };
 template <typename SP, int PXB, int PW, int TY, int V>
 struct RowPairs {
   static constexpr int ROWB = PXB * (int)sizeof(SP);  // bytes per p/D row in shared memory
@@ -924,7 +944,7 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
     for (int c = 0; c < 3; ++c) {
       const float* qx = &sqx[ps][c][ly][lx + 2];
       const T o = Lane<V, float>::ld(qx);
-      const T dx = apply3<GEN>(ax, prev_x(qx[-1], o), GEN ? o : bcast<T>(0.f), next_x(o, qx[V]));
+      const T dx = x_stencil<GEN, (OPT & kScalarX) != 0>(ax, qx[-1], o, qx[V]);
       const T dn = Lane<V, float>::ld(&sqy[ps][c][ly][lx]);
       const T up = Lane<V, float>::ld(&sqy[ps][c][ly + 2][lx]);
       const T oy = GEN ? Lane<V, float>::ld(&sqy[ps][c][ly + 1][lx]) : bcast<T>(0.f);
@@ -945,8 +965,9 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
     t = primal_step(uj, a.factor, Lane<V, SP>::ld(RC), g);
   };
   // rest of the primal of plane j: qn = q_z(j+1)
-  auto finish_primal = [&](int j, const T (&dxy)[3], const T (&qn)[3], const T (&uj)[3], const T (&g)[3], T t) {
-    const StencilV<T> az = bcast_st<T>(adj_coef(j, nz, bdry, ihz));
+  auto finish_primal = [&](int j, const Stencil3& azs, const T (&dxy)[3], const T (&qn)[3], const T (&uj)[3],
+                           const T (&g)[3], T t) {
+    const StencilV<T> az = bcast_st<T>(azs);  // adj_coef(j, ...)
     T d[3], n[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) d[c] = vadd(dxy[c], apply3<GEN>(az, qmm[c], qm[c], qn[c]));
@@ -975,8 +996,11 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
   };
 
   // One plane step; WITH_PRIMAL: role 0 also finishes plane k-1.
-  auto step = [&](const int k, auto with_primal) {
+  // kPeel: the z stencils of interior planes (the same values fwd_coef / adj_coef give there)
+  const Stencil3 fz_int = fwd_coef(1, 3, bdry, hz), az_int = adj_coef(2, 5, bdry, ihz);
+  auto step = [&](const int k, auto with_primal, auto interior) {
     constexpr bool WP = decltype(with_primal)::value;
+    constexpr bool INT = decltype(interior)::value;  // both z stencils interior, k-1 and k+1 staged
     const int need = min(k + 1, ph);
     while (waited < need && !bad) {
       ++waited;
@@ -989,11 +1013,11 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
     const int qs = k & 1;
     const SU* Uk = ubox(k) + uo;
     const unsigned char* PD = smem + G::PD_OFF + ((k - kb) % G::NPD) * B::PD_SLOT;
-    const Stencil3 fz1 = fwd_coef(k, nz, bdry, hz);
+    const Stencil3 fz1 = INT ? fz_int : fwd_coef(k, nz, bdry, hz);
     // planes k-1 and k+1 are missing only at k = 0 and k = nz-1, where the z stencil's
     // coefficient for them is zero (every boundary type): plane k stands in for them
-    const SU* Um = ubox(k - 1 >= pl ? k - 1 : k) + uo;
-    const SU* Up = ubox(k + 1 <= ph ? k + 1 : k) + uo;
+    const SU* Um = ubox(INT || k - 1 >= pl ? k - 1 : k) + uo;
+    const SU* Up = ubox(INT || k + 1 <= ph ? k + 1 : k) + uo;
     if (role == 0) {
       // interior lanes, one block with few branches so that the compiler can interleave the
       // primal of plane k-1 with the dual of plane k; lanes outside the volume compute on the
@@ -1020,7 +1044,7 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
       auto dual_comp = [&](int c, T& p0, T& p1, T& p2) {
         const SU* u = Uk + c * UC;
         const T o = Lane<V, SU>::ld(u);
-        const T ex = apply3<GEN>(fx, prev_x(Store<SU>::sh(u - 1), o), o, next_x(o, Store<SU>::sh(u + V)));
+        const T ex = x_stencil<GEN, (OPT & kScalarX) != 0>(fx, Store<SU>::sh(u - 1), o, Store<SU>::sh(u + V));
         const T ey = apply3<GEN>(fy, Lane<V, SU>::ld(u - UXB), o, Lane<V, SU>::ld(u + UXB));
         const T ez = apply3<GEN>(fz, Lane<V, SU>::ld(Um + c * UC), o, Lane<V, SU>::ld(Up + c * UC));
         dual_row(Dk, ex, ey, ez, p0, p1, p2, a.sigma, a.wtv, wtv2);
@@ -1065,12 +1089,14 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
         bad = true;
         return;
       }
-      // cells outside the volume keep their zeros
+      // cells outside the volume keep their zeros (kNoSel: a lane outside the volume computed on
+      // the zero fill of the boxes, D = 0, so its q is already exactly zero)
       const T zero = bcast<T>(0.f);
+      const bool keep = (OPT & kNoSel) ? true : active;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        Lane<V, float>::st(&sqy[qs][c][ly + 1][lx], active ? qyo[c] : zero);
-        Lane<V, float>::st(&sqx[qs][c][ly][lx + 2], active ? qxo[c] : zero);
+        Lane<V, float>::st(&sqy[qs][c][ly + 1][lx], keep ? qyo[c] : zero);
+        Lane<V, float>::st(&sqx[qs][c][ly][lx + 2], keep ? qxo[c] : zero);
       }
       if constexpr (AS) mbar_arrive(qpub + ((k - kb) & 1));
       if constexpr (WP) {
@@ -1082,7 +1108,7 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
           load_dxy(k - 1, dxy);
           primal_pre(k - 1, uo1, gp, tp);
         }
-        if (active && !bad) finish_primal(k - 1, dxy, qc, uo1, gp, tp);
+        if (active && !bad) finish_primal(k - 1, INT ? az_int : adj_coef(k - 1, nz, bdry, ihz), dxy, qc, uo1, gp, tp);
       }
     } else {
       T qyo[3];
@@ -1169,8 +1195,15 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
   // the first one or two steps have no finished plane (j = k-1 < z0)
   const int kp = min(z0 + 1, ke + 1);
   int k = kb;
-  for (; k < kp && !bad; ++k) step(k, std::false_type{});
-  for (; k <= ke && !bad; ++k) step(k, std::true_type{});
+  for (; k < kp && !bad; ++k) step(k, std::false_type{}, std::false_type{});
+  if constexpr ((OPT & kPeel) != 0) {
+    // interior steps: 1 <= k <= nz-2 (forward stencil) and j = k-1 interior for the adjoint
+    // (MIRROR: 2 <= j <= nz-3; the other boundaries: 1 <= j <= nz-2)
+    const int ilo = max(kp, GEN ? 2 : 3), ihi = min(ke, nz - 2);
+    for (; k < ilo && k <= ke && !bad; ++k) step(k, std::true_type{}, std::false_type{});
+    for (; k <= ihi && !bad; ++k) step(k, std::true_type{}, std::true_type{});
+  }
+  for (; k <= ke && !bad; ++k) step(k, std::true_type{}, std::false_type{});
   if (bad) {
     if constexpr (AS) {
       *abort_flag = 1;
@@ -1196,7 +1229,7 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
       const T zero[3] = {bcast<T>(0.f), bcast<T>(0.f), bcast<T>(0.f)};
       load_dxy(j, dxy);
       primal_pre(j, uj, g, t);
-      finish_primal(j, dxy, zero, uj, g, t);
+      finish_primal(j, adj_coef(j, nz, bdry, ihz), dxy, zero, uj, g, t);
     }
   }
 }
@@ -1238,20 +1271,17 @@ constexpr SplitShape kSplitShapes[] = {
     {32, 16, 3, 1, 1, false, 0, 0, kAllStorages}, {40, 8, 3, 1, 2, false, 0, 0, kAllStorages},
     {40, 8, 3, 2, 2, true, 0, 0, kAllStorages},   {32, 8, 3, 2, 2, true, 0, 0, kAllStorages},
     {16, 16, 3, 1, 2, true, 0, 0, kAllStorages},  {32, 16, 3, 2, 1, true, 0, 0, kAllStorages},
-    // three CTAs per SM (5.5 warps each, 72.6 KB / 66.8 KB of shared memory with 16-bit fields)
-    {16, 16, 2, 2, 3, false, 112, 0, kAllStorages}, {32, 8, 2, 2, 3, false, 112, 0, kAllStorages},
-    // two CTAs per SM with the 16x16 tile (no partial tiles at widths that are multiples of 16)
-    {16, 16, 3, 2, 2, false, 0, 0, kAllStorages},
-    // schedule and placement options (FP32 and f16-flow32 storage)
-    {40, 8, 3, 2, 2, false, 0, kJitDual, kF32AndF16Flow32},
-    {40, 8, 3, 2, 2, false, 0, kJitDual | kLatePrimal, kF32AndF16Flow32},
-    {16, 16, 2, 2, 3, false, 112, kJitDual | kLatePrimal, kF32AndF16Flow32},
-    {32, 16, 3, 2, 1, false, 0, kJitDual, kF32AndF16Flow32},
+    // placement and schedule options of the 40x8 pair-lane shape (and of the FP32 32x16 and the
+    // 16x16 shapes), FP32 and f16-flow32 storage
     {40, 8, 3, 2, 2, false, 0, kRowPairs, kF32AndF16Flow32},
     {40, 8, 3, 2, 2, false, 0, kRowPairs | (8 << 8), kF32AndF16Flow32},
-    {40, 8, 3, 2, 2, false, 0, kRowPairs | kJitDual, kF32AndF16Flow32},
-    {32, 8, 2, 2, 3, false, 112, kRowPairs | kJitDual | kLatePrimal, kF32AndF16Flow32},
-    {32, 16, 3, 2, 1, false, 0, kRowPairs, kF32AndF16Flow32}};
+    {40, 8, 3, 2, 2, false, 0, kRowPairs | kScalarX, kF32AndF16Flow32},
+    {40, 8, 3, 2, 2, false, 0, kRowPairs | kNoSel, kF32AndF16Flow32},
+    {40, 8, 3, 2, 2, false, 0, kRowPairs | kPeel, kF32AndF16Flow32},
+    {40, 8, 3, 2, 2, false, 0, kRowPairs | kScalarX | kNoSel | kPeel, kF32AndF16Flow32},
+    {40, 8, 3, 2, 2, false, 0, kRowPairs | kScalarX | kNoSel | kPeel | kJitDual | kLatePrimal, kF32AndF16Flow32},
+    {32, 16, 3, 2, 1, false, 0, kScalarX | kNoSel | kPeel, kF32AndF16Flow32},
+    {16, 16, 3, 2, 2, false, 0, kScalarX | kNoSel | kPeel, kF32AndF16Flow32}};
 constexpr int kNumSplitShapes = sizeof(kSplitShapes) / sizeof(kSplitShapes[0]);
 
 // Split-role variant `idx` for a storage mode. op 0: set the kernels' shared-memory attribute

@@ -55,7 +55,7 @@ constexpr TileShape kTileShapes[] = {
     split_entry(12),       split_entry(13),       split_entry(14),       split_entry(15),
     split_entry(16),       split_entry(17),       split_entry(18),       split_entry(19),
     split_entry(20),       split_entry(21),       split_entry(22),       split_entry(23),
-    split_entry(24),       split_entry(25),       split_entry(26),       split_entry(27)};
+    split_entry(24)};
 constexpr bool split_table_complete() {
   int n = 0;
   for (const TileShape& t : kTileShapes) n += t.form == kSplit;

@@ -64,13 +64,13 @@ bool dispatch(int idx, int op, bool gen, unsigned nt, const Tile* tiles, const D
               const IterArgs* a, int* status, cudaStream_t s, int* box) {
 #define SVS_SPLIT(I) \
   case I: return run<SU, SP, I>(op, gen, nt, tiles, descs, maps, a, status, s, box);
-  static_assert(kNumSplitShapes == 28, "one case per compiled shape");
+  static_assert(kNumSplitShapes == 25, "one case per compiled shape");
   switch (idx) {
     SVS_SPLIT(0) SVS_SPLIT(1) SVS_SPLIT(2) SVS_SPLIT(3) SVS_SPLIT(4) SVS_SPLIT(5)
     SVS_SPLIT(6) SVS_SPLIT(7) SVS_SPLIT(8) SVS_SPLIT(9) SVS_SPLIT(10) SVS_SPLIT(11)
     SVS_SPLIT(12) SVS_SPLIT(13) SVS_SPLIT(14) SVS_SPLIT(15) SVS_SPLIT(16) SVS_SPLIT(17)
     SVS_SPLIT(18) SVS_SPLIT(19) SVS_SPLIT(20) SVS_SPLIT(21) SVS_SPLIT(22) SVS_SPLIT(23)
-    SVS_SPLIT(24) SVS_SPLIT(25) SVS_SPLIT(26) SVS_SPLIT(27)
+    SVS_SPLIT(24)
     default: return false;
   }
 #undef SVS_SPLIT
