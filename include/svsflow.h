@@ -290,6 +290,16 @@ svs_status svs_tvl1_plan_check(svs_plan* plan);
  * svs_tvl1_plan_check reports SVS_ERR_TIMEOUT; the context stays usable. level, cta or plane < 0
  * switches the stall off (wait_us still applies). */
 svs_status svs_tvl1_plan_set_stall_test(svs_plan* plan, int level, int cta, int plane, uint32_t wait_us);
+/* Persistent iteration loop (no counterpart in the reference, whose tvl13d.py:213-253 launches
+ * every operator of every iteration): with on != 0, each warp of a level whose pairs all use one
+ * split-role variant that has the persistent form runs its max_outer_iterations iterations in ONE
+ * cooperative launch of the resident CTAs, which take the level's column tiles in turn and meet
+ * at a grid barrier (bounded wait, SVS_DEV_TIMEOUT on expiry) after every iteration; results are
+ * bitwise those of the per-iteration launches. Levels without the form, or a device where the
+ * cooperative launch cannot be captured into the solve's graph, keep per-iteration launches. */
+svs_status svs_tvl1_plan_set_persistent(svs_plan* plan, int on);
+/* 1 if the captured solve graph runs level `level` with the persistent loop, else 0. */
+int svs_tvl1_plan_level_persistent(const svs_plan* plan, int level);
 
 /* Allocation-free solve of ONE frame pair, for callers that cannot call cudaMalloc: code whose
  * device memory belongs to another allocator (a framework's caching pool that has reserved the

@@ -98,6 +98,8 @@ _SIGS = {
     "svs_tvl1_chunk_plan": (c_int, [c_int64, c_int, c_int64, c_void_p, c_void_p, c_void_p]),
     "svs_tvl1_plan_check": (c_int, [c_void_p]),
     "svs_tvl1_plan_set_stall_test": (c_int, [c_void_p, c_int, c_int, c_int, ctypes.c_uint32]),
+    "svs_tvl1_plan_set_persistent": (c_int, [c_void_p, c_int]),
+    "svs_tvl1_plan_level_persistent": (c_int, [c_void_p, c_int]),
     "svs_tvl1_solve_noalloc": (c_int, [ctypes.POINTER(TVL1Params), c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
 }
 

@@ -771,10 +771,13 @@ struct RowPairs {
                              ((PW - 16) * TY) % 32 == 0;
   static constexpr int NPAIRED = 16 * TY;  // lanes placed in row pairs; the rest row by row
 };
+// What split_body did with its tile: skipped it (the pair had stopped; shared memory untouched),
+// finished it, or gave up at a timed-out pipeline wait (the same in every thread of the CTA).
+enum { kItemSkipped = 0, kItemDone = 1, kItemTimeout = 2 };
 template <typename SU, typename SP, int TX, int TY, int DIST, int V, bool GEN, bool AS, int OPT = 0>
-__device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const Desc* __restrict__ descs,
-                                           const TMaps* __restrict__ maps, const IterArgs a,
-                                           int* __restrict__ status) {
+__device__ __forceinline__ int split_body(const Tile* __restrict__ tiles, const int item,
+                                           const Desc* __restrict__ descs, const TMaps* __restrict__ maps,
+                                           const IterArgs a, int* __restrict__ status) {
   using G = SplitGeom<SU, SP, TX, TY, DIST, V, AS, (OPT >> 8)>;
   using B = typename G::B;
   using T = LaneT<V>;
@@ -786,9 +789,9 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
   float(*sqy)[3][TY + 2][TX] = reinterpret_cast<float(*)[3][TY + 2][TX]>(smem + G::SQY_OFF);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + G::BAR_OFF);
 
-  const Tile Tl = tiles[blockIdx.x];
+  const Tile Tl = tiles[item];
   const Desc& Dg = descs[Tl.desc];
-  if (Dg.stop && *Dg.stop) return;  // pair converged for this level
+  if (Dg.stop && *Dg.stop) return kItemSkipped;  // pair converged for this level
   const TMaps* M = maps + Tl.desc;
   const int nz = Dg.nz, ny = Dg.ny, nx = Dg.nx;
   const int cs = (int)Dg.cs;
@@ -854,7 +857,7 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
   const int kb = max(z0 - 1, 0), ke = min(z1, nz - 1);
   const int pl = max(kb - 1, 0), ph = min(ke + 1, nz - 1);
   const uint64_t wait_ns = (uint64_t)a.wait_us * 1000ull;
-  const int stall_r = (int)blockIdx.x == a.stall_cta ? a.stall_plane : -1;
+  const int stall_r = item == a.stall_cta ? a.stall_plane : -1;
   auto issue = [&](int q) {
     const int r = q - pl;
     if (r == stall_r) return;  // timeout-path test: this plane's copies are never issued
@@ -919,7 +922,7 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
           }
         }
       }
-      return;
+      return kItemDone;
     }
   } else {
     if (tid == 0) {
@@ -1216,13 +1219,13 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
         mbar_wait(bars + r % G::NB, (uint32_t)((r / G::NB) & 1), wait_ns);
       }
     }
-    return;
+    return kItemTimeout;
   }
   if (z1 >= nz) {
     const int j = nz - 1;
     if (AS && role == 0 && !wait_q(j)) {
       atomicOr(status, SVS_DEV_TIMEOUT);
-      return;
+      return kItemTimeout;
     }
     if (role == 0 && active && j >= z0) {
       T dxy[3], uj[3], g[3], t;
@@ -1232,6 +1235,7 @@ __device__ __forceinline__ void split_body(const Tile* __restrict__ tiles, const
       finish_primal(j, adj_coef(j, nz, bdry, ihz), dxy, zero, uj, g, t);
     }
   }
+  return kItemDone;
 }
 
 // The split-role kernel with a register budget for MINB resident CTAs per SM (launch bounds)...
@@ -1239,7 +1243,7 @@ template <typename SU, typename SP, int TX, int TY, int DIST, int V, int MINB, b
 __global__ void __launch_bounds__(SplitGeom<SU, SP, TX, TY, DIST, V, AS>::NT_LAUNCH, MINB)
 iterate_split_kernel(const Tile* __restrict__ tiles, const Desc* __restrict__ descs,
                      const TMaps* __restrict__ maps, IterArgs a, int* __restrict__ status) {
-  split_body<SU, SP, TX, TY, DIST, V, GEN, AS, OPT>(tiles, descs, maps, a, status);
+  split_body<SU, SP, TX, TY, DIST, V, GEN, AS, OPT>(tiles, blockIdx.x, descs, maps, a, status);
 }
 // ...or with an explicit per-thread register cap: the launch-bounds arithmetic rounds a block of
 // 5.5 warps up further than the register file requires, so three 176-thread CTAs per SM (6
@@ -1248,7 +1252,85 @@ template <typename SU, typename SP, int TX, int TY, int DIST, int V, int REGS, b
 __global__ void __launch_bounds__(SplitGeom<SU, SP, TX, TY, DIST, V, AS>::NT_LAUNCH) __maxnreg__(REGS)
 iterate_split_kernel_r(const Tile* __restrict__ tiles, const Desc* __restrict__ descs,
                        const TMaps* __restrict__ maps, IterArgs a, int* __restrict__ status) {
-  split_body<SU, SP, TX, TY, DIST, V, GEN, AS, OPT>(tiles, descs, maps, a, status);
+  split_body<SU, SP, TX, TY, DIST, V, GEN, AS, OPT>(tiles, blockIdx.x, descs, maps, a, status);
+}
+
+// ------------------------------------------------------------- persistent iteration loop
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+// Generic-proxy stores of this thread are ordered before later async-proxy (TMA) accesses.
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+// Barrier over every CTA of a co-resident (cooperative) grid. The arrival counter starts at zero
+// and grows by gridDim.x per use, so use number g waits for g * gridDim.x arrivals. Bounded:
+// thread 0 gives up after limit_ns and the call returns false in every thread of the CTA.
+__device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned target, uint64_t limit_ns) {
+  int ok = 1;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(counter, 1u);
+    const uint64_t t0 = global_ns();
+    while (ld_acquire_gpu(counter) < target) {
+      if (global_ns() - t0 > limit_ns) {
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    fence_proxy_async_global();  // this thread issues the next copies, after the acquire
+  }
+  return __syncthreads_and(ok) != 0;
+}
+
+// All iterations of one warp at one level in one launch: the resident CTAs (a cooperative grid)
+// take the level's column tiles in turn (tile blockIdx.x, blockIdx.x + gridDim.x, ...), run each
+// exactly as iterate_split_kernel does, and meet at a grid barrier after every iteration, the
+// tiles of iteration it+1 reading the ping-pong copies iteration it wrote. The schedule of sigma
+// and tau per iteration is the host's (tvl13d.py:240-249); the arithmetic per voxel is that of
+// the per-iteration launches, so the result is bitwise the same.
+template <typename SU, typename SP, int TX, int TY, int DIST, int V, int MINB, bool GEN, int OPT = 0>
+__global__ void __launch_bounds__(SplitGeom<SU, SP, TX, TY, DIST, V, false>::NT_LAUNCH, MINB)
+iterate_persist_kernel(const Tile* __restrict__ tiles, int ntiles, const Desc* __restrict__ descs,
+                       const TMaps* __restrict__ maps, PersistArgs pa, int* __restrict__ status) {
+  using G = SplitGeom<SU, SP, TX, TY, DIST, V, false, (OPT >> 8)>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + G::BAR_OFF);
+  const uint64_t limit = (uint64_t)pa.wait_us * 1000ull;
+  for (int it = 0; it < pa.iters; ++it) {
+    IterArgs a;
+    a.sigma = pa.sig[it];
+    a.tau = pa.tau[it];
+    a.factor = __fmul_rn(a.tau, pa.wm);  // opticalFlowOps.cu:440, as the host computes it
+    a.wtv = pa.wtv;
+    a.src = (pa.src0 + it) & 1;
+    a.bdry = pa.bdry;
+    a.wait_us = pa.wait_us;
+    a.stall_cta = pa.stall_cta;
+    a.stall_plane = pa.stall_plane;
+    for (int item = blockIdx.x; item < ntiles; item += gridDim.x) {
+      const int r = split_body<SU, SP, TX, TY, DIST, V, GEN, false, OPT>(tiles, item, descs, maps, a, status);
+      // the item's shared memory (rings, q rows, mbarriers) is free again; after a timed-out
+      // pipeline wait this CTA stops, and the others then time out at the grid barrier
+      __syncthreads();
+      if (r == kItemTimeout) return;
+      if (r == kItemDone && threadIdx.x == 0)
+        for (int b = 0; b < G::NB; ++b) mbar_inval(bars + b);
+    }
+    // this iteration's stores (generic proxy) come before any CTA's copies of the next one
+    fence_proxy_async_global();
+    if (!grid_barrier(pa.counter, (unsigned)(it + 1) * gridDim.x, limit)) {
+      if (threadIdx.x == 0) atomicOr(status, SVS_DEV_TIMEOUT);
+      return;
+    }
+  }
 }
 
 // Compiled shapes of the split-role form (tile, prefetch distance, voxels per lane, CTAs per SM
@@ -1276,7 +1358,7 @@ constexpr SplitShape kSplitShapes[] = {
     {40, 8, 3, 2, 2, false, 0, kRowPairs, kF32AndF16Flow32},
     {40, 8, 3, 2, 2, false, 0, kRowPairs | (8 << 8), kF32AndF16Flow32},
     {40, 8, 3, 2, 2, false, 0, kRowPairs | kScalarX, kF32AndF16Flow32},
-    {40, 8, 3, 2, 2, false, 0, kRowPairs | kNoSel, kF32AndF16Flow32},
+    {40, 8, 3, 2, 2, false, 0, kRowPairs | kNoSel, kAllStorages},  // the 16-bit default at widths of 40
     {40, 8, 3, 2, 2, false, 0, kRowPairs | kPeel, kF32AndF16Flow32},
     {40, 8, 3, 2, 2, false, 0, kRowPairs | kScalarX | kNoSel | kPeel, kF32AndF16Flow32},
     {40, 8, 3, 2, 2, false, 0, kRowPairs | kScalarX | kNoSel | kPeel | kJitDual | kLatePrimal, kF32AndF16Flow32},
@@ -1290,5 +1372,31 @@ constexpr int kNumSplitShapes = sizeof(kSplitShapes) / sizeof(kSplitShapes[0]);
 // in box[0] (after op 0).
 bool split_variant(int storage, int idx, int op, bool gen, unsigned ntiles, const Tile* tiles, const Desc* descs,
                    const TMaps* maps, const IterArgs* a, int* status, cudaStream_t s, int* box);
+
+template <typename SU, typename SP> constexpr int storage_id() {
+  if constexpr (std::is_same<SU, float>::value && std::is_same<SP, float>::value) return SVS_STORAGE_F32;
+  else if constexpr (std::is_same<SU, float>::value && std::is_same<SP, __half>::value) return SVS_STORAGE_F16_FLOW32;
+  else if constexpr (std::is_same<SU, float>::value) return SVS_STORAGE_BF16_FLOW32;
+  else if constexpr (std::is_same<SP, __half>::value) return SVS_STORAGE_F16;
+  else return SVS_STORAGE_BF16;
+}
+
+// The shapes that also have the persistent form (iterate_persist_kernel): those the automatic
+// per-level choice uses (32x16 pairs, 40x8 pairs in row pairs, 32x8 and 16x16 single voxels) and
+// the 32x8 pair shape, at prefetch distance 3, block barrier per plane, every storage mode.
+constexpr bool has_persist(const SplitShape& S) {
+  if (S.as || S.regs != 0 || S.dist != 3 || S.smask != kAllStorages) return false;
+  if (S.opt == (kRowPairs | kNoSel)) return S.tx == 40 && S.ty == 8 && S.v == 2;
+  if (S.opt != 0) return false;
+  return (S.tx == 32 && S.ty == 16 && S.v == 2) || (S.tx == 32 && S.ty == 8 && S.v == 2 && S.minb == 1) ||
+         (S.tx == 32 && S.ty == 8 && S.v == 1) || (S.tx == 16 && S.ty == 16 && S.v == 1);
+}
+
+// Persistent launch of split-role variant `idx`: all `pa->iters` iterations of one warp at one
+// level over `ntiles` tiles, one cooperative grid of the resident CTAs. op 0: set the kernels'
+// shared-memory attribute; op 1: launch on stream s. False if the variant has no persistent form
+// (has_persist) or the launch failed.
+bool split_persist(int storage, int idx, int op, bool gen, unsigned ntiles, const Tile* tiles, const Desc* descs,
+                   const TMaps* maps, const PersistArgs* pa, int* status, cudaStream_t s);
 
 }  // namespace svs

@@ -593,6 +593,12 @@ struct svs_plan {
   // bounded pipeline waits (svs_tvl1_plan_set_stall_test)
   unsigned wait_us = 2000000;
   int stall_level = -1, stall_cta = -1, stall_plane = -1;
+  // persistent iteration loop (svs_tvl1_plan_set_persistent): one cooperative launch per warp
+  bool persistent = false;
+  std::vector<char> level_persist;         // per level: the persistent form is used
+  float* d_sig = nullptr;                  // [max_outer_iterations] schedule on the device
+  float* d_tau = nullptr;
+  unsigned* d_gridbar = nullptr;           // grid-barrier arrival counter
 };
 
 namespace svs {
@@ -738,23 +744,25 @@ bool iter_dispatch(svs_plan& P, std::vector<TMaps>* maps, int level, int tid, in
   }
 }
 
-constexpr int split_id(int tx, int ty, int dist, int v) {
+constexpr int split_id(int tx, int ty, int dist, int v, int opt = 0) {
   for (int i = 0; i < kNumTileShapes; ++i)
     if (kTileShapes[i].form == kSplit && kTileShapes[i].tx == tx && kTileShapes[i].ty == ty &&
         kTileShapes[i].dist == dist && kSplitShapes[kTileShapes[i].split].v == v &&
-        !kSplitShapes[kTileShapes[i].split].as)
+        !kSplitShapes[kTileShapes[i].split].as && kSplitShapes[kTileShapes[i].split].opt == opt &&
+        kSplitShapes[kTileShapes[i].split].smask == kAllStorages)
       return i + 1;
   return 0;
 }
 constexpr int kAutoF32 = split_id(32, 16, 3, 2), kAuto16 = split_id(16, 16, 3, 1),
-              kAuto16W40 = split_id(40, 8, 3, 2), kAuto16Narrow = split_id(32, 8, 3, 1);
+              kAuto16W40 = split_id(40, 8, 3, 2, kRowPairs | kNoSel), kAuto16Narrow = split_id(32, 8, 3, 1);
 static_assert(kAutoF32 > 0 && kAuto16 > 0 && kAuto16W40 > 0 && kAuto16Narrow > 0,
               "automatic variants are compiled");
 
 // Automatic choice per level (measured on B200 with batches of 80^3 pairs, levels 80^3, 40^3 and
 // 20^3): split-role pipelines with prefetch distance 3. 4-byte fields: 32x16 tiles of voxel
 // pairs (one CTA per SM). 2-byte fields: 40x8 tiles of voxel pairs when every width is a
-// multiple of 40 (no idle lanes), 32x8 tiles of single voxels for widths up to 32, 16x16 tiles
+// multiple of 40 (no idle lanes; interior lanes placed in row pairs, which halves the shared-
+// memory bank conflicts), 32x8 tiles of single voxels for widths up to 32, 16x16 tiles
 // of single voxels otherwise. The plain-load 32x8 form if TMA descriptors cannot be built. The
 // autotuner measures instead of assuming.
 int auto_tile(const svs_plan& P, int level) {
@@ -927,6 +935,14 @@ svs_status setup_tiles(svs_plan& P) {
     }
     P.pair_mask = nullptr;
   }
+  // persistent iteration loop: levels whose pairs share one split-role variant that has the form
+  P.level_persist.assign(P.levels, 0);
+  for (int l = 0; l < P.levels && P.persistent; ++l) {
+    const TileShape& ts = kTileShapes[P.level_tile[l] - 1];
+    P.level_persist[l] = P.extra[l].empty() && ts.form == kSplit && !P.h_tiles[l].empty() &&
+                         split_persist(P.prm.storage, ts.split, 0, P.prm.boundary != SVS_BOUNDARY_MIRROR, 0, nullptr,
+                                       nullptr, nullptr, nullptr, nullptr, nullptr);
+  }
   for (auto* p : P.d_tiles) cudaFree(p);
   P.d_tiles.assign(P.levels, nullptr);
   size_t widest = 0;
@@ -1062,13 +1078,36 @@ long long enqueue_solve(svs_plan& P, cudaStream_t s) {
     for (int w = 0; w < q.max_warps; ++w) {
       linearise_kernel<SU, SP><<<grid(l), 256, 0, s>>>(D + (size_t)l * np, cur, q.interpolation, q.boundary);
       ++launches;
-      fork_groups(P, l, s);
-      for (int it = 0; it < q.max_outer_iterations; ++it) {
-        const IterArgs a = iter_args(P, it, cur);
-        launches += level_iteration(P, l, a, s);
-        cur ^= 1;
+      if (l < (int)P.level_persist.size() && P.level_persist[l] && q.max_outer_iterations > 0) {
+        // every iteration of the warp in one cooperative launch (grid barrier between them)
+        PersistArgs pa;
+        pa.sig = P.d_sig;
+        pa.tau = P.d_tau;
+        pa.wm = P.prm.weight_matching;
+        pa.wtv = P.prm.weight_tv;
+        pa.src0 = cur;
+        pa.bdry = P.prm.boundary;
+        pa.iters = q.max_outer_iterations;
+        pa.wait_us = P.wait_us;
+        pa.stall_cta = l == P.stall_level ? P.stall_cta : -1;
+        pa.stall_plane = l == P.stall_level ? P.stall_plane : -1;
+        pa.counter = P.d_gridbar;
+        cudaMemsetAsync(P.d_gridbar, 0, sizeof(unsigned), s);
+        const TileShape& ts = kTileShapes[P.level_tile[l] - 1];
+        if (!split_persist(P.prm.storage, ts.split, 1, q.boundary != SVS_BOUNDARY_MIRROR,
+                           (unsigned)P.h_tiles[l].size(), P.d_tiles[l], P.d_descs, P.d_maps, &pa, P.d_status, s))
+          return -1;
+        ++launches;
+        cur ^= q.max_outer_iterations & 1;
+      } else {
+        fork_groups(P, l, s);
+        for (int it = 0; it < q.max_outer_iterations; ++it) {
+          const IterArgs a = iter_args(P, it, cur);
+          launches += level_iteration(P, l, a, s);
+          cur ^= 1;
+        }
+        join_groups(P, l, s);
       }
-      join_groups(P, l, s);
       if (P.res_on) {
         residual_kernel<SU><<<grid(l), 256, 0, s>>>(D + (size_t)l * np, cur, P.d_snaps, P.d_acc, 0);
         residual_finish_kernel<<<ceil_div(np, 128), 128, 0, s>>>(D + (size_t)l * np, P.d_acc, P.d_reslog, L,
@@ -1276,7 +1315,18 @@ svs_status svs_tvl1_plan_create(const svs_tvl1_params* prm, int num_pairs, const
     for (size_t i = 0; i < k3.size(); ++i) P->blur.w[i] = k3[i] / tot;
     P->blur_r = ks / 2;
   }
-  st = check_cuda(cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking), "svs_tvl1_plan_create");
+  // the schedule again on the device, for the persistent iteration loop, and its barrier counter
+  const size_t nsch = std::max<size_t>(1, P->sig_sched.size());
+  st = check_cuda(cudaMalloc((void**)&P->d_sig, nsch * sizeof(float)), "svs_tvl1_plan_create");
+  if (!st) st = check_cuda(cudaMalloc((void**)&P->d_tau, nsch * sizeof(float)), "svs_tvl1_plan_create");
+  if (!st) st = check_cuda(cudaMalloc((void**)&P->d_gridbar, sizeof(unsigned)), "svs_tvl1_plan_create");
+  if (!st && !P->sig_sched.empty())
+    st = check_cuda(cudaMemcpy(P->d_sig, P->sig_sched.data(), P->sig_sched.size() * sizeof(float), cudaMemcpyHostToDevice),
+                    "svs_tvl1_plan_create");
+  if (!st && !P->tau_sched.empty())
+    st = check_cuda(cudaMemcpy(P->d_tau, P->tau_sched.data(), P->tau_sched.size() * sizeof(float), cudaMemcpyHostToDevice),
+                    "svs_tvl1_plan_create");
+  if (!st) st = check_cuda(cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking), "svs_tvl1_plan_create");
   if (st) { svs_tvl1_plan_destroy(P); return st; }
   *out = P;
   return SVS_OK;
@@ -1290,6 +1340,7 @@ svs_status svs_tvl1_plan_destroy(svs_plan* P) {
   cudaFree(P->d_descs); cudaFree(P->d_raw); cudaFree(P->d_uout); cudaFree(P->d_umed);
   cudaFree(P->d_pout); cudaFree(P->d_uinit); cudaFree(P->d_pinit); cudaFree(P->d_maps);
   cudaFree(P->d_status);
+  cudaFree(P->d_sig); cudaFree(P->d_tau); cudaFree(P->d_gridbar);
   for (auto& lv : P->extra)
     for (auto& grp : lv) cudaFree(grp.d);
   for (cudaStream_t st_ : P->side) cudaStreamDestroy(st_);
@@ -1434,8 +1485,22 @@ svs_status svs_tvl1_solve_batch(svs_plan* P, const svs_pair_desc* pairs, int num
     cudaGraph_t g = nullptr;
     st = check_cuda(cudaStreamBeginCapture(P->cap_stream, cudaStreamCaptureModeThreadLocal), "solve: capture");
     if (st) return st;
-    const long long nl = enqueue(*P, P->cap_stream);
-    const cudaError_t ce = cudaStreamEndCapture(P->cap_stream, &g);
+    long long nl = enqueue(*P, P->cap_stream);
+    cudaError_t ce = cudaStreamEndCapture(P->cap_stream, &g);
+    if ((nl < 0 || ce != cudaSuccess) && P->persistent) {
+      // the cooperative launch of the persistent loop could not be captured here: per-iteration
+      // launches instead (svs_tvl1_plan_level_persistent then reports 0)
+      if (g) cudaGraphDestroy(g);
+      g = nullptr;
+      cudaGetLastError();
+      P->persistent = false;
+      st = setup_tiles(*P);
+      if (st) return st;
+      st = check_cuda(cudaStreamBeginCapture(P->cap_stream, cudaStreamCaptureModeThreadLocal), "solve: capture");
+      if (st) return st;
+      nl = enqueue(*P, P->cap_stream);
+      ce = cudaStreamEndCapture(P->cap_stream, &g);
+    }
     if (nl < 0) { if (g) cudaGraphDestroy(g); return fail(SVS_ERR_LAUNCH, std::string("solve: launch failed during capture: ") + cudaGetErrorString(cudaGetLastError())); }
     st = check_cuda(ce, "solve: end capture");
     if (st) return st;
@@ -1517,6 +1582,19 @@ svs_status svs_tvl1_plan_check(svs_plan* P) {
   }
   if (flags & SVS_DEV_TIMEOUT) return fail(SVS_ERR_TIMEOUT, "a pipeline wait in the iterate kernel timed out; results are invalid");
   return SVS_OK;
+}
+
+svs_status svs_tvl1_plan_set_persistent(svs_plan* P, int on) {
+  SVS_REQUIRE(P, "svs_tvl1_plan_set_persistent: null plan");
+  P->persistent = on != 0;
+  ++P->tile_epoch;  // rebuild the per-level choice and recapture the graph
+  return SVS_OK;
+}
+
+int svs_tvl1_plan_level_persistent(const svs_plan* P, int level) {
+  return (P && level >= 0 && level < (int)P->level_persist.size() && P->graph_tile == P->tile_epoch)
+             ? (int)P->level_persist[level]
+             : 0;
 }
 
 svs_status svs_tvl1_plan_set_stall_test(svs_plan* P, int level, int cta, int plane, uint32_t wait_us) {

@@ -6,14 +6,6 @@
 namespace svs {
 namespace {
 
-template <typename SU, typename SP> constexpr int storage_id() {
-  if constexpr (std::is_same<SU, float>::value && std::is_same<SP, float>::value) return SVS_STORAGE_F32;
-  else if constexpr (std::is_same<SU, float>::value && std::is_same<SP, __half>::value) return SVS_STORAGE_F16_FLOW32;
-  else if constexpr (std::is_same<SU, float>::value) return SVS_STORAGE_BF16_FLOW32;
-  else if constexpr (std::is_same<SP, __half>::value) return SVS_STORAGE_F16;
-  else return SVS_STORAGE_BF16;
-}
-
 template <typename SU, typename SP, int I>
 bool run(int op, bool gen, unsigned nt, const Tile* tiles, const Desc* descs, const TMaps* maps,
          const IterArgs* a, int* status, cudaStream_t s, int* box) {

@@ -99,6 +99,19 @@ struct IterArgs {
   int stall_cta, stall_plane;
 };
 
+// The persistent form of the iteration loop: all `iters` primal-dual iterations of one warp at
+// one level in a single cooperative launch (svs_iterate.cuh, iterate_persist_kernel).
+struct PersistArgs {
+  const float* sig;    // [iters] sigma of each iteration (device; the host float64 schedule rounded)
+  const float* tau;    // [iters] tau of each iteration
+  float wm, wtv;       // weight_matching (factor = tau * wm), weight_tv
+  int src0, bdry;      // ping-pong copy read by the first iteration; boundary type
+  int iters;
+  unsigned wait_us;    // bound of every pipeline and grid-barrier wait
+  int stall_cta, stall_plane;  // the timeout-path test of IterArgs (stall_cta counts tiles)
+  unsigned* counter;   // grid-barrier arrivals, zero at launch
+};
+
 // TMA descriptors of one (pair, level): the two ping-pong copies of u and p, D, rc and gw.
 struct alignas(64) TMaps {
   CUtensorMap u[2];

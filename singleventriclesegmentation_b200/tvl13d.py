@@ -79,6 +79,15 @@ class SolverPlan:
         check() then raises with SVS_ERR_TIMEOUT. No arguments switch the stall off."""
         check(_lib.lib().svs_tvl1_plan_set_stall_test(self._h, int(level), int(cta), int(plane), int(wait_us)))
 
+    def set_persistent(self, on: bool = True) -> None:
+        """Run each warp's iterations of a level in one cooperative launch (grid barrier between
+        iterations) where the level's variant has that form; the result is bitwise unchanged."""
+        check(_lib.lib().svs_tvl1_plan_set_persistent(self._h, int(bool(on))))
+
+    def level_persistent(self, levels: int = 3):
+        """Per level, whether the captured solve runs the persistent loop (after a solve)."""
+        return [bool(_lib.lib().svs_tvl1_plan_level_persistent(self._h, l)) for l in range(levels)]
+
     def level_tiles(self):
         return [int(_lib.lib().svs_tvl1_plan_level_tile(self._h, l)) for l in range(8)]
 
