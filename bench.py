@@ -69,7 +69,7 @@ def parse():
     ap.add_argument("--rates", default="0.1,1,10,50", help="serving: arrival rates (requests/s)")
     ap.add_argument("--reps", type=int, default=50, help="latency: repetitions of the single-pair solve")
     ap.add_argument("--requests", type=int, default=6, help="serving: requests per rate")
-    ap.add_argument("--max-active", type=int, default=2, help="serving: requests on the device at once")
+    ap.add_argument("--max-active", type=int, default=0, help="serving: cap on admitted requests (0: the HBM budget alone)")
     return ap.parse_args()
 
 
@@ -532,7 +532,7 @@ def run_serving(args):
             masks = torch.from_numpy(np.stack([synthetic.ellipsoid_mask(dims, (15, 12, 10)),
                                                synthetic.ellipsoid_mask(dims, (13, 12, 10))])).pin_memory()
             data.append((frames, masks, (0, min(12, T - 1))))
-        server = FlowServer(budget_bytes=100 << 30, storage=storage, device=dev, max_active=args.max_active)
+        server = FlowServer(budget_bytes=100 << 30, storage=storage, device=dev, max_active=args.max_active or None)
         t0 = time.perf_counter()
         futs = []
         for (ta, _, _), (frames, masks, mt) in zip(reqs, data):
@@ -551,6 +551,7 @@ def run_serving(args):
                         "mean_s": st["mean_s"], "throughput_seq_per_s": st["throughput_seq_per_s"],
                         "throughput_pairs_per_s": pairs / span,
                         "throughput_80cube_equiv_pairs_per_s": eq80 / span, "max_concurrent": st["max_concurrent"],
+                        "batches": st["batches"], "mixed_batches": st["mixed_batches"],
                         "sizes": [[T] + list(d) for _, T, d in reqs]})
     print(json.dumps({"metric": "serving: per-sequence latency p50/p99 and throughput", "unit": "s",
                       "storage": storage, "data": "synthetic", "budget_bytes": 100 << 30,

@@ -255,6 +255,21 @@ svs_status svs_tvl1_plan_get_residuals(svs_plan* plan, float* out_host, size_t c
  * autotuner and tests). */
 svs_status svs_tvl1_tile_info(int tile_id, int* tx, int* ty, int* dist, int* form, int* lane_voxels);
 
+/* A plan sized by capacity for svs_tvl1_plan_retarget (no counterpart in the reference): room for
+ * up to max_pairs pairs and at least arena_bytes of device state (the per-pair state of a level-0
+ * voxel is about 190 bytes with 16-bit fields, 290 with FP32 storage, three scales). It starts
+ * with a placeholder batch of max_pairs small cubes; retarget it before solving. */
+svs_status svs_tvl1_plan_create_reserve(const svs_tvl1_params* params, int max_pairs, size_t arena_bytes,
+                                        svs_plan** plan);
+/* Re-use a plan for another batch without allocating (no counterpart in the reference): the plan
+ * takes num_pairs pairs with level-0 sizes dims_host[3i..3i+2], num_pairs at most its pair count
+ * at creation and their device state at most its arena (SVS_ERR_OUT_OF_MEMORY otherwise); state
+ * is cleared on `stream`, tile lists, tensor maps and the solve graph are rebuilt at the next
+ * solve, per-pair variant requests are dropped. Not with residuals on. The plan must not be
+ * solving on any stream. Used by the serving loop, which packs pairs of several requests into
+ * one batch. */
+svs_status svs_tvl1_plan_retarget(svs_plan* plan, int num_pairs, const int* dims_host, svs_stream_t stream);
+
 /* Solve every pair of the plan (pairs[i] must match dims[i] of the plan). */
 svs_status svs_tvl1_solve_batch(svs_plan* plan, const svs_pair_desc* pairs_host, int num_pairs,
                                 svs_stream_t stream);

@@ -99,6 +99,8 @@ _SIGS = {
     "svs_tvl1_plan_check": (c_int, [c_void_p]),
     "svs_tvl1_plan_set_stall_test": (c_int, [c_void_p, c_int, c_int, c_int, ctypes.c_uint32]),
     "svs_tvl1_plan_set_persistent": (c_int, [c_void_p, c_int]),
+    "svs_tvl1_plan_retarget": (c_int, [c_void_p, c_int, ctypes.POINTER(c_int), c_void_p]),
+    "svs_tvl1_plan_create_reserve": (c_int, [ctypes.POINTER(TVL1Params), c_int, c_size_t, ctypes.POINTER(c_void_p)]),
     "svs_tvl1_plan_level_persistent": (c_int, [c_void_p, c_int]),
     "svs_tvl1_solve_noalloc": (c_int, [ctypes.POINTER(TVL1Params), c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
 }

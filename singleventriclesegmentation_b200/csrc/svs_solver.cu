@@ -532,6 +532,7 @@ __global__ void warm_start_kernel(const Desc* __restrict__ descs, const float* c
 struct svs_plan {
   svs_tvl1_params prm{};
   int num_pairs = 0;
+  int capacity = 0;                        // pairs the device tables hold (svs_tvl1_plan_retarget)
   int levels = 0;
   std::vector<int> dims;                   // level-0 dims, 3 per pair
   std::vector<svs::Desc> h_descs;          // [levels][pairs]
@@ -1156,6 +1157,74 @@ template <typename T> T* carve(char*& cur, size_t count) {
   return p;
 }
 
+// Mesh sizes per level (tvl13d.py:91-99, ceil halving), spacings (coreDefines.h:72-75) and the
+// device bytes of a batch of `n` pairs with level-0 sizes dims[3i..3i+2]; descs gets
+// [levels][n] descriptors without device pointers.
+svs_status layout_batch(const svs_plan& P, int n, const int* dims, std::vector<Desc>& descs, size_t& bytes) {
+  const svs_tvl1_params& prm = P.prm;
+  descs.assign((size_t)P.levels * n, Desc{});
+  bytes = 0;
+  const size_t ub = flow_bytes(prm.storage), sb = field_bytes(prm.storage);
+  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+  for (int i = 0; i < n; ++i) {
+    int nz = dims[3 * i], ny = dims[3 * i + 1], nx = dims[3 * i + 2];
+    if (nz >= 65535 || ny >= 65535 || nx >= 65535) return fail(SVS_ERR_INVALID_ARG, "plan: volume dimension too large");
+    for (int l = 0; l < P.levels; ++l) {
+      if (l > 0) { nz = (nz + 1) / 2; ny = (ny + 1) / 2; nx = (nx + 1) / 2; }
+      if (nz < 3 || ny < 3 || nx < 3)
+        return fail(SVS_ERR_INVALID_ARG, "plan: every pyramid level needs at least 3 nodes per axis");
+      Desc& d = descs[(size_t)l * n + i];
+      std::memset(&d, 0, sizeof(d));
+      d.nz = nz; d.ny = ny; d.nx = nx;
+      d.pitch = (nx + 7) / 8 * 8;
+      d.n = (long long)nz * ny * nx;
+      d.cs = (long long)d.pitch * ny * nz;
+      if (prm.length_type == 0) { d.lz = (float)(nz - 1); d.ly = (float)(ny - 1); d.lx = (float)(nx - 1); }
+      else { d.lz = prm.length_z; d.ly = prm.length_y; d.lx = prm.length_x; }
+      d.hz = d.lz / (float)(nz - 1); d.hy = d.ly / (float)(ny - 1); d.hx = d.lx / (float)(nx - 1);
+      const size_t nv = (size_t)d.n, cs = (size_t)d.cs;
+      bytes += 2 * al(nv * 4) + al(4 * nv * 4);                      // I0, I1, ig
+      bytes += al(6 * cs * sb) + al(cs * sb) + al(3 * cs * sb);      // D, rc, gw
+      bytes += 2 * al(3 * cs * ub) + 2 * al(9 * cs * sb);            // u[2], p[2]
+      if (9 * cs >= (size_t)1 << 31) return fail(SVS_ERR_INVALID_ARG, "plan: volume too large for 32-bit field offsets");
+      if (l == 0) bytes += 2 * al(nv * 4) + 2 * al(3 * nv * 4) + al(9 * nv * 4);  // raw x2, uout, umed, pout
+    }
+  }
+  bytes += 4096;
+  return SVS_OK;
+}
+
+// Device pointers of P.h_descs ([levels][num_pairs]) and the per-pair buffers, carved from the arena.
+void carve_batch(svs_plan& P) {
+  const int n = P.num_pairs;
+  const size_t ub = flow_bytes(P.prm.storage), sb = field_bytes(P.prm.storage);
+  char* cur = reinterpret_cast<char*>(P.arena);
+  P.raw.assign(2 * n, nullptr); P.uout.assign(n, nullptr); P.pout.assign(n, nullptr); P.umed.assign(n, nullptr);
+  P.uinit.assign(n, nullptr); P.pinit.assign(n, nullptr);
+  for (int l = 0; l < P.levels; ++l)
+    for (int i = 0; i < n; ++i) {
+      Desc& d = P.h_descs[(size_t)l * n + i];
+      const size_t nv = (size_t)d.n, cs = (size_t)d.cs;
+      d.I0 = carve<float>(cur, nv);
+      d.I1 = carve<float>(cur, nv);
+      d.ig = carve<float>(cur, 4 * nv);
+      d.D = carve<char>(cur, 6 * cs * sb);
+      d.rc = carve<char>(cur, cs * sb);
+      d.gw = carve<char>(cur, 3 * cs * sb);
+      d.u[0] = carve<char>(cur, 3 * cs * ub);
+      d.u[1] = carve<char>(cur, 3 * cs * ub);
+      d.p[0] = carve<char>(cur, 9 * cs * sb);
+      d.p[1] = carve<char>(cur, 9 * cs * sb);
+      if (l == 0) {
+        P.raw[2 * i] = carve<float>(cur, nv);
+        P.raw[2 * i + 1] = carve<float>(cur, nv);
+        P.uout[i] = carve<float>(cur, 3 * nv);
+        P.umed[i] = carve<float>(cur, 3 * nv);
+        P.pout[i] = carve<float>(cur, 9 * nv);
+      }
+    }
+}
+
 }  // namespace
 }  // namespace svs
 
@@ -1193,72 +1262,20 @@ svs_status svs_tvl1_plan_create(const svs_tvl1_params* prm, int num_pairs, const
               "svs_tvl1_plan_create: median kernel must be 0, 1, 3, 5 or 7");
   svs_plan* P = new svs_plan();
   P->prm = *prm;
-  P->num_pairs = num_pairs;
   P->levels = prm->num_scales;
-  P->dims.assign(dims, dims + 3 * num_pairs);
-  // mesh sizes per level (tvl13d.py:91-99, ceil halving) and spacings (coreDefines.h:72-75)
-  P->h_descs.resize((size_t)P->levels * num_pairs);
   size_t bytes = 0;
-  const size_t ub = flow_bytes(prm->storage), sb = field_bytes(prm->storage);
-  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
-  for (int i = 0; i < num_pairs; ++i) {
-    int nz = dims[3 * i], ny = dims[3 * i + 1], nx = dims[3 * i + 2];
-    if (nz >= 65535 || ny >= 65535 || nx >= 65535) { delete P; return fail(SVS_ERR_INVALID_ARG, "svs_tvl1_plan_create: volume dimension too large"); }
-    for (int l = 0; l < P->levels; ++l) {
-      if (l > 0) { nz = (nz + 1) / 2; ny = (ny + 1) / 2; nx = (nx + 1) / 2; }
-      if (nz < 3 || ny < 3 || nx < 3) {
-        delete P;
-        return fail(SVS_ERR_INVALID_ARG, "svs_tvl1_plan_create: every pyramid level needs at least 3 nodes per axis");
-      }
-      Desc& d = P->h_descs[(size_t)l * num_pairs + i];
-      std::memset(&d, 0, sizeof(d));
-      d.nz = nz; d.ny = ny; d.nx = nx;
-      d.pitch = (nx + 7) / 8 * 8;
-      d.n = (long long)nz * ny * nx;
-      d.cs = (long long)d.pitch * ny * nz;
-      if (prm->length_type == 0) { d.lz = (float)(nz - 1); d.ly = (float)(ny - 1); d.lx = (float)(nx - 1); }
-      else { d.lz = prm->length_z; d.ly = prm->length_y; d.lx = prm->length_x; }
-      d.hz = d.lz / (float)(nz - 1); d.hy = d.ly / (float)(ny - 1); d.hx = d.lx / (float)(nx - 1);
-      const size_t n = (size_t)d.n, cs = (size_t)d.cs;
-      bytes += 2 * al(n * 4) + al(4 * n * 4);                       // I0, I1, ig
-      bytes += al(6 * cs * sb) + al(cs * sb) + al(3 * cs * sb);      // D, rc, gw
-      bytes += 2 * al(3 * cs * ub) + 2 * al(9 * cs * sb);            // u[2], p[2]
-      if (9 * cs >= (size_t)1 << 31) { delete P; return fail(SVS_ERR_INVALID_ARG, "svs_tvl1_plan_create: volume too large for 32-bit field offsets"); }
-      if (l == 0) bytes += 2 * al(n * 4) + 2 * al(3 * n * 4) + al(9 * n * 4);  // raw x2, uout, umed, pout
-    }
-  }
-  bytes += 4096;
-  svs_status st = check_cuda(cudaMalloc(&P->arena, bytes), "svs_tvl1_plan_create: device state");
+  svs_status st = layout_batch(*P, num_pairs, dims, P->h_descs, bytes);
+  if (st) { delete P; return st; }
+  P->num_pairs = num_pairs;
+  P->capacity = num_pairs;
+  P->dims.assign(dims, dims + 3 * num_pairs);
+  st = check_cuda(cudaMalloc(&P->arena, bytes), "svs_tvl1_plan_create: device state");
   if (st) { delete P; return st; }
   P->arena_bytes = bytes;
   // zero the whole arena once: pitch padding and planes never written stay zero
   st = check_cuda(cudaMemset(P->arena, 0, bytes), "svs_tvl1_plan_create");
   if (st) { svs_tvl1_plan_destroy(P); return st; }
-  char* cur = reinterpret_cast<char*>(P->arena);
-  P->raw.resize(2 * num_pairs); P->uout.resize(num_pairs); P->pout.resize(num_pairs); P->umed.resize(num_pairs);
-  P->uinit.assign(num_pairs, nullptr); P->pinit.assign(num_pairs, nullptr);
-  for (int l = 0; l < P->levels; ++l)
-    for (int i = 0; i < num_pairs; ++i) {
-      Desc& d = P->h_descs[(size_t)l * num_pairs + i];
-      const size_t n = (size_t)d.n, cs = (size_t)d.cs;
-      d.I0 = carve<float>(cur, n);
-      d.I1 = carve<float>(cur, n);
-      d.ig = carve<float>(cur, 4 * n);
-      d.D = carve<char>(cur, 6 * cs * sb);
-      d.rc = carve<char>(cur, cs * sb);
-      d.gw = carve<char>(cur, 3 * cs * sb);
-      d.u[0] = carve<char>(cur, 3 * cs * ub);
-      d.u[1] = carve<char>(cur, 3 * cs * ub);
-      d.p[0] = carve<char>(cur, 9 * cs * sb);
-      d.p[1] = carve<char>(cur, 9 * cs * sb);
-      if (l == 0) {
-        P->raw[2 * i] = carve<float>(cur, n);
-        P->raw[2 * i + 1] = carve<float>(cur, n);
-        P->uout[i] = carve<float>(cur, 3 * n);
-        P->umed[i] = carve<float>(cur, 3 * n);
-        P->pout[i] = carve<float>(cur, 9 * n);
-      }
-    }
+  carve_batch(*P);
   auto upload = [&](void** dptr, const void* src, size_t sz) -> svs_status {
     svs_status s2 = check_cuda(cudaMalloc(dptr, sz), "svs_tvl1_plan_create");
     if (s2) return s2;
@@ -1581,6 +1598,87 @@ svs_status svs_tvl1_plan_check(svs_plan* P) {
     if (st) return st;
   }
   if (flags & SVS_DEV_TIMEOUT) return fail(SVS_ERR_TIMEOUT, "a pipeline wait in the iterate kernel timed out; results are invalid");
+  return SVS_OK;
+}
+
+svs_status svs_tvl1_plan_create_reserve(const svs_tvl1_params* prm, int max_pairs, size_t arena_bytes,
+                                        svs_plan** out) {
+  SVS_REQUIRE(prm && out, "svs_tvl1_plan_create_reserve: null pointer");
+  SVS_REQUIRE(max_pairs > 0, "svs_tvl1_plan_create_reserve: max_pairs must be positive");
+  SVS_REQUIRE(prm->num_scales >= 1 && prm->num_scales <= 8, "svs_tvl1_plan_create_reserve: num_scales out of range");
+  // a placeholder batch: max_pairs of the smallest cube every level of the pyramid accepts
+  const int side = 3 << (prm->num_scales - 1);
+  std::vector<int> dims((size_t)3 * max_pairs, side);
+  svs_plan* P = nullptr;
+  svs_status st = svs_tvl1_plan_create(prm, max_pairs, dims.data(), &P);
+  if (st) return st;
+  if (arena_bytes > P->arena_bytes) {
+    void* bigger = nullptr;
+    st = check_cuda(cudaMalloc(&bigger, arena_bytes), "svs_tvl1_plan_create_reserve: device state");
+    if (!st) st = check_cuda(cudaMemset(bigger, 0, arena_bytes), "svs_tvl1_plan_create_reserve");
+    if (st) {
+      cudaFree(bigger);
+      svs_tvl1_plan_destroy(P);
+      return st;
+    }
+    cudaFree(P->arena);
+    P->arena = bigger;
+    P->arena_bytes = arena_bytes;
+    carve_batch(*P);
+    st = check_cuda(cudaMemcpy(P->d_descs, P->h_descs.data(), P->h_descs.size() * sizeof(Desc), cudaMemcpyHostToDevice),
+                    "svs_tvl1_plan_create_reserve");
+    if (!st) st = check_cuda(cudaMemcpy(P->d_raw, P->raw.data(), P->raw.size() * sizeof(float*), cudaMemcpyHostToDevice),
+                             "svs_tvl1_plan_create_reserve");
+    if (!st) st = check_cuda(cudaMemcpy(P->d_uout, P->uout.data(), P->uout.size() * sizeof(float*), cudaMemcpyHostToDevice),
+                             "svs_tvl1_plan_create_reserve");
+    if (!st) st = check_cuda(cudaMemcpy(P->d_umed, P->umed.data(), P->umed.size() * sizeof(float*), cudaMemcpyHostToDevice),
+                             "svs_tvl1_plan_create_reserve");
+    if (st) {
+      svs_tvl1_plan_destroy(P);
+      return st;
+    }
+  }
+  *out = P;
+  return SVS_OK;
+}
+
+svs_status svs_tvl1_plan_retarget(svs_plan* P, int num_pairs, const int* dims, svs_stream_t stream) {
+  SVS_REQUIRE(P && dims, "svs_tvl1_plan_retarget: null pointer");
+  SVS_REQUIRE(num_pairs > 0 && num_pairs <= P->capacity,
+              "svs_tvl1_plan_retarget: num_pairs must be positive and at most the plan's pair count at creation");
+  SVS_REQUIRE(!P->res_on, "svs_tvl1_plan_retarget: not with residuals on (their buffers are sized per pair)");
+  std::vector<Desc> descs;
+  size_t bytes = 0;
+  svs_status st = layout_batch(*P, num_pairs, dims, descs, bytes);
+  if (st) return st;
+  if (bytes > P->arena_bytes)
+    return fail(SVS_ERR_OUT_OF_MEMORY, "svs_tvl1_plan_retarget: the batch needs " + std::to_string(bytes) +
+                                           " bytes of device state; the plan holds " + std::to_string(P->arena_bytes));
+  cudaStream_t s = stream;
+  P->num_pairs = num_pairs;
+  P->dims.assign(dims, dims + 3 * num_pairs);
+  P->h_descs = std::move(descs);
+  carve_batch(*P);
+  // clear the state the batch uses (as at creation), then the tables (descriptors with the stop
+  // flags off, pointer arrays; the caller's output pointers are filled by each solve)
+  st = check_cuda(cudaMemsetAsync(P->arena, 0, bytes, s), "svs_tvl1_plan_retarget");
+  if (!st) st = check_cuda(cudaMemcpyAsync(P->d_descs, P->h_descs.data(), P->h_descs.size() * sizeof(Desc),
+                                           cudaMemcpyHostToDevice, s), "svs_tvl1_plan_retarget");
+  if (!st) st = check_cuda(cudaMemcpyAsync(P->d_raw, P->raw.data(), P->raw.size() * sizeof(float*), cudaMemcpyHostToDevice, s),
+                           "svs_tvl1_plan_retarget");
+  if (!st) st = check_cuda(cudaMemcpyAsync(P->d_uout, P->uout.data(), P->uout.size() * sizeof(float*), cudaMemcpyHostToDevice, s),
+                           "svs_tvl1_plan_retarget");
+  if (!st) st = check_cuda(cudaMemcpyAsync(P->d_umed, P->umed.data(), P->umed.size() * sizeof(float*), cudaMemcpyHostToDevice, s),
+                           "svs_tvl1_plan_retarget");
+  std::vector<float*> nop((size_t)num_pairs, nullptr);
+  if (!st) st = check_cuda(cudaMemcpyAsync(P->d_pout, nop.data(), nop.size() * sizeof(float*), cudaMemcpyHostToDevice, s),
+                           "svs_tvl1_plan_retarget");
+  if (!st) st = check_cuda(cudaStreamSynchronize(s), "svs_tvl1_plan_retarget");  // the host tables may change now
+  if (st) return st;
+  P->want_p = false;
+  P->warm = false;
+  P->pair_tile_req.clear();  // pair indices of the earlier batch mean nothing now
+  ++P->tile_epoch;           // tiles, tensor maps and the graph follow the new sizes
   return SVS_OK;
 }
 

@@ -37,6 +37,23 @@ class SolverPlan:
                                                   ctypes.byref(handle)))
         self._h = handle
 
+    @classmethod
+    def reserve(cls, params: TVL1Params, max_pairs: int, arena_bytes: int, device: torch.device) -> "SolverPlan":
+        """A plan with room for up to max_pairs pairs and arena_bytes of device state, to be
+        retarget()ed to each batch (svs_tvl1_plan_create_reserve)."""
+        self = cls.__new__(cls)
+        self.device = device
+        self.params = params
+        handle = ctypes.c_void_p()
+        with torch.cuda.device(device):
+            check(_lib.lib().svs_tvl1_plan_create_reserve(ctypes.byref(params), int(max_pairs), int(arena_bytes),
+                                                          ctypes.byref(handle)))
+        self._h = handle
+        side = 3 << (params.num_scales - 1)
+        self.dims = [(side, side, side)] * int(max_pairs)
+        self.capacity = int(max_pairs)
+        return self
+
     @property
     def device_bytes(self) -> int:
         return int(_lib.lib().svs_tvl1_plan_device_bytes(self._h))
@@ -78,6 +95,16 @@ class SolverPlan:
         of its staged plane number `plane`, and waits give up after wait_us (0 = 2 s); the next
         check() then raises with SVS_ERR_TIMEOUT. No arguments switch the stall off."""
         check(_lib.lib().svs_tvl1_plan_set_stall_test(self._h, int(level), int(cta), int(plane), int(wait_us)))
+
+    def retarget(self, dims: Sequence[Tuple[int, int, int]], stream=None) -> None:
+        """Take another batch (at most as many pairs as at creation, state within the arena)
+        without allocating; synchronizes `stream`."""
+        dims = [tuple(int(v) for v in d) for d in dims]
+        arr = (ctypes.c_int * (3 * len(dims)))(*[v for d in dims for v in d])
+        s = stream if stream is not None else stream_ptr(self.device)
+        with torch.cuda.device(self.device):
+            check(_lib.lib().svs_tvl1_plan_retarget(self._h, len(dims), arr, s))
+        self.dims = dims
 
     def set_persistent(self, on: bool = True) -> None:
         """Run each warp's iterations of a level in one cooperative launch (grid barrier between

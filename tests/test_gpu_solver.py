@@ -281,3 +281,31 @@ def test_in_solve_median_equals_post_filter(cuda, pair24):
     u = s1.compute_batch([T(I0)], [T(I1)])[0]
     um = s2.compute_batch([T(I0)], [T(I1)])[0]
     assert torch.equal(apply_median_filter(u, 3), um)
+
+
+def test_retargeted_plan_equals_fresh_plans(cuda):
+    """svs_tvl1_plan_retarget / svs_tvl1_plan_create_reserve: a plan re-used for batches of other
+    sizes (fewer pairs, state within its arena) gives bitwise the results of plans made for those
+    batches, and refuses a batch it cannot hold."""
+    from singleventriclesegmentation_b200 import _lib
+    from singleventriclesegmentation_b200.tvl13d import SolverPlan
+    solver, _ = make_solver(storage="f16-flow32", max_warps=2, max_outer_iterations=20)
+    batches = [[(24, 24, 24), (20, 28, 32)], [(32, 32, 32)], [(16, 16, 24)] * 3]
+    reserved = SolverPlan.reserve(solver.params(), 4, 600 << 20, torch.device("cuda"))
+    for b, dims in enumerate(batches):
+        pairs = [synthetic.frame_pair(d, seed=40 + 3 * b + i) for i, d in enumerate(dims)]
+        I0s, I1s = [T(p[0]) for p in pairs], [T(p[1]) for p in pairs]
+        ref = solver.compute_batch(I0s, I1s)
+        reserved.retarget(dims)
+        outs = [torch.empty(d + (3,), device="cuda") for d in dims]
+        reserved.solve(I0s, I1s, outs)
+        reserved.check()
+        for a, o in zip(ref, outs):
+            assert torch.equal(a, o)
+    with pytest.raises(_lib.SVSError) as e:
+        reserved.retarget([(24, 24, 24)] * 5)   # more pairs than at creation
+    assert e.value.status == 1
+    with pytest.raises(_lib.SVSError) as e:
+        reserved.retarget([(256, 256, 256)])    # more state than the arena
+    assert e.value.status == 2
+    reserved.close()
