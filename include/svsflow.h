@@ -283,6 +283,19 @@ svs_status svs_tvl1_bench_iterations(svs_plan* plan, int level, int count, svs_s
 uint64_t svs_tvl1_plan_graph_kernels(const svs_plan* plan);
 /* Iterate-kernel variant the plan uses at a pyramid level (after the first solve; 0 before). */
 int svs_tvl1_plan_level_tile(const svs_plan* plan, int level);
+/* Variant one pair runs at a pyramid level: the level's, or its group's (requested with
+ * svs_tvl1_plan_set_pair_tile or chosen automatically); after the first solve, 0 before. */
+int svs_tvl1_plan_pair_tile_used(const svs_plan* plan, int level, int pair);
+/* The automatic variant choice for one pyramid level, host arithmetic only (no counterpart in
+ * the reference): num_pairs sizes dims_host[3i..3i+2] = (nz, ny, nx) at that level, storage mode,
+ * SM count. Returns the level's variant and writes pair_tile_out[i] = pair i's own variant where
+ * it differs (0: the level's); 0 for invalid arguments. 2-byte fields at levels whose 40x8
+ * column tiles fill two CTAs per SM at least twice: each pair takes the variant with the least
+ * work (column tiles x planes x a measured time per column-tile plane) and the variant with the
+ * most work is the level's; otherwise one variant per level (FP32 fields: 32x16 voxel pairs;
+ * 2-byte fields: 40x8 voxel pairs when every width is a multiple of 40, 32x8 single voxels up to
+ * width 32, 16x16 single voxels otherwise). */
+int svs_tvl1_auto_tiles(int storage, int num_pairs, const int* dims_host, int sms, int* pair_tile_out);
 /* CTAs of one iteration at a pyramid level, all variant groups together (after the first solve;
  * 0 before): the column tiles times their z chunks. */
 int64_t svs_tvl1_plan_level_ctas(const svs_plan* plan, int level);

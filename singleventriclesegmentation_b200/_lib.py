@@ -94,6 +94,8 @@ _SIGS = {
     "svs_tvl1_bench_iterations": (c_int, [c_void_p, c_int, c_int, c_void_p]),
     "svs_tvl1_plan_graph_kernels": (ctypes.c_uint64, [c_void_p]),
     "svs_tvl1_plan_level_tile": (c_int, [c_void_p, c_int]),
+    "svs_tvl1_plan_pair_tile_used": (c_int, [c_void_p, c_int, c_int]),
+    "svs_tvl1_auto_tiles": (c_int, [c_int, c_int, ctypes.POINTER(c_int), c_int, ctypes.POINTER(c_int)]),
     "svs_tvl1_plan_level_ctas": (c_int64, [c_void_p, c_int]),
     "svs_tvl1_chunk_plan": (c_int, [c_int64, c_int, c_int64, c_void_p, c_void_p, c_void_p]),
     "svs_tvl1_plan_check": (c_int, [c_void_p]),
@@ -164,6 +166,18 @@ def tile_info(tile_id: int) -> dict:
     check(lib().svs_tvl1_tile_info(int(tile_id), *[ctypes.byref(x) for x in v]))
     return {"tx": v[0].value, "ty": v[1].value, "dist": v[2].value,
             "form": ("plain", "tma", "split")[v[3].value], "lane_voxels": v[4].value}
+
+
+def auto_tiles(storage: int, dims, sms: int):
+    """The automatic iterate-kernel choice for one pyramid level (host arithmetic): `dims` are the
+    pairs' (nz, ny, nx) at that level. Returns (level variant, [pair variant or 0 per pair])."""
+    n = len(dims)
+    arr = (c_int * (3 * n))(*[int(v) for d in dims for v in d])
+    out = (c_int * max(n, 1))()
+    main = int(lib().svs_tvl1_auto_tiles(int(storage), n, arr, int(sms), out))
+    if main == 0:
+        raise SVSError(1, "svs_tvl1_auto_tiles: invalid arguments")
+    return main, [int(out[i]) for i in range(n)]
 
 
 def chunk_plan(columns: int, nz: int, slots: int) -> dict:

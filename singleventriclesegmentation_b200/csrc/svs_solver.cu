@@ -541,6 +541,7 @@ struct svs_plan {
   std::vector<std::vector<svs::Tile>> h_tiles;  // per level
   std::vector<svs::Tile*> d_tiles;
   std::vector<int> level_tile;             // tile id used per level
+  std::vector<std::vector<int>> pair_used; // tile id used per level and pair (groups included)
   std::vector<int> level_tile_req;         // per-level request (0 = use tile_id)
   std::vector<int> level_chunks_req;       // per-level z chunks per column (0 = the wave model)
   int tile_id = 0;                         // requested for all levels (0 = automatic)
@@ -759,24 +760,82 @@ constexpr int kAutoF32 = split_id(32, 16, 3, 2), kAuto16 = split_id(16, 16, 3, 1
 static_assert(kAutoF32 > 0 && kAuto16 > 0 && kAuto16W40 > 0 && kAuto16Narrow > 0,
               "automatic variants are compiled");
 
-// Automatic choice per level (measured on B200 with batches of 80^3 pairs, levels 80^3, 40^3 and
-// 20^3): split-role pipelines with prefetch distance 3. 4-byte fields: 32x16 tiles of voxel
-// pairs (one CTA per SM). 2-byte fields: 40x8 tiles of voxel pairs when every width is a
-// multiple of 40 (no idle lanes; interior lanes placed in row pairs, which halves the shared-
-// memory bank conflicts), 32x8 tiles of single voxels for widths up to 32, 16x16 tiles
-// of single voxels otherwise. The plain-load 32x8 form if TMA descriptors cannot be built. The
-// autotuner measures instead of assuming.
-int auto_tile(const svs_plan& P, int level) {
-  if (P.prm.storage == SVS_STORAGE_F32) return kAutoF32;
+// Automatic choice per level from the level's sizes (nz, ny, nx per pair), the storage mode and
+// the SM count; host arithmetic only. Returns the level's variant; pair_tid[i] is pair i's own
+// variant where it differs (0: the level's).
+//
+// Levels whose column tiles do not fill the GPU twice over (measured on B200 with batches of 80^3
+// pairs, levels 80^3, 40^3 and 20^3): split-role pipelines with prefetch distance 3. 4-byte
+// fields: 32x16 tiles of voxel pairs (one CTA per SM). 2-byte fields: 40x8 tiles of voxel pairs
+// when every width is a multiple of 40 (no idle lanes; interior lanes placed in row pairs, which
+// halves the shared-memory bank conflicts), 32x8 tiles of single voxels for widths up to 32, 16x16
+// tiles of single voxels otherwise.
+//
+// 2-byte fields at levels that fill the GPU at least twice (the iteration time is then the work of
+// all tiles, not the latency of one z march): each pair takes the variant with the least work,
+// column tiles x planes x the variant's time per column-tile plane at full occupancy (measured on
+// B200 at level 0 of 68-128 pairs of 64^3-128^3); the variant with the most work becomes the
+// level's, the others run as groups of pairs (parallel branches of the graph).
+//
+// The plain-load 32x8 form if TMA descriptors cannot be built. The autotuner measures instead of
+// assuming.
+struct AutoCost {
+  int tid;
+  float ns;  // per column-tile plane
+};
+// 40x8 voxel pairs in row pairs 6.22-6.42 ns (320 voxels), 32x8 voxel pairs 5.01-5.14 ns (256
+// voxels), 16x16 single voxels 6.11-6.19 ns (256 voxels): per voxel the first two are alike
+// (~20 ps) and the third 20% slower
+constexpr AutoCost kAutoCosts16[] = {{kAuto16W40, 6.35f}, {split_id(32, 8, 3, 2), 5.10f}, {kAuto16, 6.15f}};
+constexpr int kAutoWaves = 2;  // waves of 40x8 column tiles (two CTAs per SM) for the per-pair choice
+
+int auto_choice(int storage, int n, const int* dims, int sms, int* pair_tid) {
+  for (int i = 0; i < n; ++i) pair_tid[i] = 0;
+  if (storage == SVS_STORAGE_F32) return kAutoF32;
   bool all40 = true;
   int widest = 0;
-  for (int i = 0; i < P.num_pairs; ++i) {
-    const int nx = P.h_descs[(size_t)level * P.num_pairs + i].nx;
+  long long cols = 0;
+  for (int i = 0; i < n; ++i) {
+    const int ny = dims[3 * i + 1], nx = dims[3 * i + 2];
     all40 = all40 && nx % 40 == 0;
     widest = std::max(widest, nx);
+    cols += (long long)ceil_div(nx, 40) * ceil_div(ny, 8);
   }
-  if (all40) return kAuto16W40;
-  return widest <= 32 ? kAuto16Narrow : kAuto16;
+  const int base = all40 ? kAuto16W40 : widest <= 32 ? kAuto16Narrow : kAuto16;
+  if (n < 1 || cols < (long long)kAutoWaves * 2 * std::max(sms, 1)) return base;
+  std::vector<double> work(kNumTileShapes + 1, 0.0);
+  for (int i = 0; i < n; ++i) {
+    const int nz = dims[3 * i], ny = dims[3 * i + 1], nx = dims[3 * i + 2];
+    double best = -1.0;
+    for (const AutoCost& c : kAutoCosts16) {
+      const TileShape& ts = kTileShapes[c.tid - 1];
+      const double w = (double)ceil_div(nx, ts.tx) * ceil_div(ny, ts.ty) * nz * c.ns;
+      if (best < 0 || w < best) {
+        best = w;
+        pair_tid[i] = c.tid;
+      }
+    }
+    work[pair_tid[i]] += best;
+  }
+  const int main_tid = (int)(std::max_element(work.begin(), work.end()) - work.begin());
+  for (int i = 0; i < n; ++i)
+    if (pair_tid[i] == main_tid) pair_tid[i] = 0;
+  return main_tid;
+}
+
+int auto_level(const svs_plan& P, int level, std::vector<int>& pair_tid) {
+  std::vector<int> dims(3 * (size_t)P.num_pairs);
+  for (int i = 0; i < P.num_pairs; ++i) {
+    const Desc& d = P.h_descs[(size_t)level * P.num_pairs + i];
+    dims[3 * i] = d.nz;
+    dims[3 * i + 1] = d.ny;
+    dims[3 * i + 2] = d.nx;
+  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  pair_tid.assign(P.num_pairs, 0);
+  return auto_choice(P.prm.storage, P.num_pairs, dims.data(), sms, pair_tid.data());
 }
 
 // z chunks per column for a split-role variant. The launch's CTAs are dispatched in tile-list
@@ -890,6 +949,7 @@ svs_status setup_tiles(svs_plan& P) {
   const int want = P.tile_id;
   P.h_tiles.assign(P.levels, {});
   P.level_tile.assign(P.levels, 0);
+  P.pair_used.assign(P.levels, {});
   for (auto& lv : P.extra)
     for (auto& grp : lv) cudaFree(grp.d);
   P.extra.assign(P.levels, {});
@@ -897,11 +957,29 @@ svs_status setup_tiles(svs_plan& P) {
   std::memset(maps.data(), 0, maps.size() * sizeof(TMaps));
   for (int l = 0; l < P.levels; ++l) {
     const int req = (l < (int)P.level_tile_req.size() && P.level_tile_req[l] > 0) ? P.level_tile_req[l] : want;
-    int tid = req > 0 ? req : auto_tile(P, l);
-    // per-pair requests that differ from the level's variant form groups of their own
+    std::vector<int> autop;
+    int tid = req > 0 ? req : auto_level(P, l, autop);
+    // per-pair requests (and, without a level request, the automatic per-pair choices) that
+    // differ from the level's variant form groups of their own
     std::vector<int> own(P.num_pairs, 0);
     if (l < (int)P.pair_tile_req.size())
       for (int i = 0; i < P.num_pairs; ++i) own[i] = P.pair_tile_req[l][i];
+    if (req <= 0 && !autop.empty()) {
+      // an automatic group whose variant cannot be set up (shared memory or TMA descriptor
+      // limits) leaves every pair with the level's variant
+      bool usable = true;
+      for (const AutoCost& c : kAutoCosts16) {
+        std::vector<char> gm(P.num_pairs, 0);
+        bool any = false;
+        for (int i = 0; i < P.num_pairs; ++i) any |= gm[i] = !own[i] && autop[i] == c.tid;
+        if (!any) continue;
+        P.pair_mask = &gm;
+        usable = usable && iter_dispatch(P, &maps, l, c.tid, 0, nullptr, nullptr);
+      }
+      P.pair_mask = nullptr;
+      for (int i = 0; i < P.num_pairs && usable; ++i)
+        if (!own[i]) own[i] = autop[i];
+    }
     std::vector<char> mask(P.num_pairs, 1);
     for (int i = 0; i < P.num_pairs; ++i) mask[i] = own[i] == 0 || own[i] == tid;
     P.pair_mask = &mask;
@@ -935,6 +1013,9 @@ svs_status setup_tiles(svs_plan& P) {
       P.extra[l].push_back(std::move(grp));
     }
     P.pair_mask = nullptr;
+    P.pair_used[l].assign(P.num_pairs, tid);
+    for (int i = 0; i < P.num_pairs; ++i)
+      if (!mask[i]) P.pair_used[l][i] = own[i];
   }
   // persistent iteration loop: levels whose pairs share one split-role variant that has the form
   P.level_persist.assign(P.levels, 0);
@@ -1567,6 +1648,20 @@ uint64_t svs_tvl1_plan_graph_kernels(const svs_plan* P) { return P ? P->graph_ke
 
 int svs_tvl1_plan_level_tile(const svs_plan* P, int level) {
   return (P && level >= 0 && level < (int)P->level_tile.size()) ? P->level_tile[level] : 0;
+}
+
+int svs_tvl1_plan_pair_tile_used(const svs_plan* P, int level, int pair) {
+  if (!P || level < 0 || level >= (int)P->pair_used.size() || pair < 0 || pair >= (int)P->pair_used[level].size())
+    return 0;
+  return P->pair_used[level][pair];
+}
+
+int svs_tvl1_auto_tiles(int storage, int num_pairs, const int* dims_host, int sms, int* pair_tile_out) {
+  if (num_pairs < 1 || !dims_host || !pair_tile_out || storage < SVS_STORAGE_F32 || storage > SVS_STORAGE_F16_FLOW32)
+    return 0;
+  for (int i = 0; i < 3 * num_pairs; ++i)
+    if (dims_host[i] < 1) return 0;
+  return auto_choice(storage, num_pairs, dims_host, sms, pair_tile_out);
 }
 
 svs_status svs_tvl1_chunk_plan(int64_t columns, int nz, int64_t slots, int* main_chunks, int* tail_chunks,

@@ -118,6 +118,10 @@ class SolverPlan:
     def level_tiles(self):
         return [int(_lib.lib().svs_tvl1_plan_level_tile(self._h, l)) for l in range(8)]
 
+    def pair_tiles(self, level: int):
+        """Variant each pair runs at `level` (its group's or the level's; after a solve)."""
+        return [int(_lib.lib().svs_tvl1_plan_pair_tile_used(self._h, int(level), i)) for i in range(len(self.dims))]
+
     def level_ctas(self, level: int) -> int:
         """CTAs of one iterate launch at `level` (all variant groups; 0 before the first solve)."""
         return int(_lib.lib().svs_tvl1_plan_level_ctas(self._h, int(level)))

@@ -105,3 +105,38 @@ def test_chunk_plan_of_the_split_kernels():
                 assert _plan_cost(cols, nz, slots, p) <= best_uniform
     with pytest.raises(_lib.SVSError):
         _lib.chunk_plan(0, 80, 296)
+
+
+def test_automatic_variant_choice():
+    """The automatic per-level choice (host arithmetic, no GPU). The 68-pair 80^3 bench: 40x8
+    voxel pairs at levels 0 and 1 and 32x8 single voxels at level 2 (20^3), one variant per level;
+    FP32 fields: 32x16 voxel pairs. A batch whose level fills the GPU with widths that are and are
+    not multiples of 40 gives each width its own variant (all pairs of one width alike, the
+    multiples of 40 on the 40x8 shape); too small a batch keeps one variant per level."""
+    def tid(tx, ty, v):
+        for t in range(1, _lib.lib().svs_tvl1_num_tiles() + 1):
+            i = _lib.tile_info(t)
+            if i["form"] == "split" and (i["tx"], i["ty"], i["lane_voxels"]) == (tx, ty, v):
+                return t
+    f16_flow32, f32 = 4, 0
+    main0, pairs0 = _lib.auto_tiles(f16_flow32, [(80, 80, 80)] * 68, 148)
+    main1, pairs1 = _lib.auto_tiles(f16_flow32, [(40, 40, 40)] * 68, 148)
+    main2, pairs2 = _lib.auto_tiles(f16_flow32, [(20, 20, 20)] * 68, 148)
+    assert main0 == main1 == 28 and _lib.tile_info(28)["tx"] == 40 and _lib.tile_info(28)["lane_voxels"] == 2
+    assert main2 == tid(32, 8, 1)
+    assert not any(pairs0 + pairs1 + pairs2)
+    mf, pf = _lib.auto_tiles(f32, [(80, 80, 80)] * 68, 148)
+    assert mf == tid(32, 16, 2) and not any(pf)
+    dims = [(n, n, n) for n in (64, 80, 96, 128, 120, 64, 80, 96, 128, 120) * 6]
+    main, pairs = _lib.auto_tiles(f16_flow32, dims, 148)
+    used = [p or main for p in pairs]
+    by_width = {}
+    for d, t in zip(dims, used):
+        by_width.setdefault(d[2], set()).add(t)
+    assert all(len(s) == 1 for s in by_width.values())
+    assert by_width[80] == by_width[120] == {28}
+    assert by_width[64] != {28} and by_width[128] != {28}
+    small_main, small_pairs = _lib.auto_tiles(f16_flow32, [(64, 64, 64), (80, 80, 80)], 148)
+    assert small_main == tid(16, 16, 1) and not any(small_pairs)
+    with pytest.raises(_lib.SVSError):
+        _lib.auto_tiles(f16_flow32, [(0, 80, 80)], 148)

@@ -184,6 +184,32 @@ def test_pair_variant_groups_run_concurrently_with_the_same_result(cuda):
     plan.check()
 
 
+def test_automatic_pair_variants_keep_the_result(cuda):
+    """At a level whose column tiles fill the GPU twice over, the automatic choice gives the pairs
+    of each width the variant with the least modelled work (svs_tvl1_auto_tiles) and the plan runs
+    them as groups; the result is bitwise that of one variant for every pair."""
+    from singleventriclesegmentation_b200 import _lib
+    shapes = [(12, 64, 64)] * 20 + [(12, 80, 80)] * 16 + [(12, 72, 96)] * 4
+    pairs = [synthetic.frame_pair(sh, seed=40 + i) for i, sh in enumerate(shapes)]
+    I0, I1 = [T(p[0]) for p in pairs], [T(p[1]) for p in pairs]
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    main, own = _lib.auto_tiles(4, shapes, sms)   # f16-flow32
+    assert len(set(o or main for o in own)) >= 2
+    solver, _ = make_solver(storage="f16-flow32", max_warps=1, max_outer_iterations=10)
+    plan = solver.plan_for(shapes)
+    outs = [torch.empty(sh + (3,), device="cuda") for sh in shapes]
+    plan.solve(I0, I1, outs)
+    torch.cuda.synchronize()
+    plan.check()
+    assert plan.level_tiles()[0] == main
+    assert plan.pair_tiles(0) == [o or main for o in own]
+    solver1, _ = make_solver(storage="f16-flow32", max_warps=1, max_outer_iterations=10)
+    solver1.tile_id = 28
+    ref = solver1.compute_batch(I0, I1)
+    for a, b in zip(ref, outs):
+        assert torch.equal(a, b)
+
+
 @pytest.mark.parametrize("storage", ["f32", "f16-flow32"])
 def test_z_chunk_overrides_keep_the_result(cuda, storage):
     """Splitting the columns of a level into more z chunks (svs_tvl1_plan_set_level_chunks, down to
