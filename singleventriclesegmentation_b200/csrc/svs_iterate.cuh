@@ -760,13 +760,13 @@ enum { kLatePrimal = 1, kJitDual = 2, kRowPairs = 4, kScalarX = 8, kNoSel = 16, 
 template <typename SP, int PXB, int PW, int TY, int V>
 struct RowPairs {
   static constexpr int ROWB = PXB * (int)sizeof(SP);  // bytes per p/D row in shared memory
-  static constexpr int pick() {
-    if (sizeof(SP) == 4) return 1;  // 8-byte accesses: any row distance is conflict-free
+  static constexpr int pick16() {
     for (int d = 1; d <= 8; d *= 2)
       if (TY % (2 * d) == 0 && (d * ROWB) % 128 == 64) return d;
     return 0;
   }
-  static constexpr int D = pick();
+  // 8-byte accesses (4-byte fields): any row distance is conflict-free
+  static constexpr int D = sizeof(SP) == 4 ? 1 : pick16();
   static constexpr bool ok = V == 2 && PW >= 16 && D > 0 && TY % (2 * (D > 0 ? D : 1)) == 0 &&
                              ((PW - 16) * TY) % 32 == 0;
   static constexpr int NPAIRED = 16 * TY;  // lanes placed in row pairs; the rest row by row
