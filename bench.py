@@ -12,7 +12,9 @@ Before warm-up the iterate-kernel variant of each pyramid level is autotuned on 
 state. Beside the headline line's contract keys it reports the plain GPU form (the reference's
 per-operator structure on this package's kernels, one 80^3 pair, full schedule) for the ratio the
 metric asks for, `latency` (p50/p99 of the 68-pair sequence from the timed steps, and of one 80^3
-pair solved alone), `fp32_storage` (the same sequence solve with every field stored in FP32) and
+pair solved alone), `fp32_storage` (the same sequence solve with every field stored in FP32),
+`persistent_form` (the same pair solves with the persistent iteration loop: one cooperative
+launch per warp and level, its graph size, and a bitwise check against the headline flows) and
 `compute_metrics` (the workload's own end-mask Dice / Hausdorff, warping.py:245-270). The
 reference arm (--impl reference) adds `reference_gpu`: the reference's own CUDA extension on one
 pair of the sequence. Further workloads, one JSON line each, on one GPU:
@@ -61,6 +63,7 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-latency", action="store_true", help="skip the single-pair latency reps")
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-storage sequence solve")
+    ap.add_argument("--no-persistent", action="store_true", help="skip the persistent-loop sequence solve")
     ap.add_argument("--frames", type=int, default=T_FRAMES)
     ap.add_argument("--workload", default="sequence", choices=["sequence", "uneven", "mixed", "serving", "latency"],
                     help="sequence: 35-frame 80^3 cine sequence (the headline line); uneven: 64 pairs of "
@@ -371,6 +374,32 @@ def fp32_storage_rate(dev, d_seq, pairs, args):
     return out
 
 
+def persistent_form_rate(dev, d_seq, pairs, storage, level_tiles, ref_host):
+    """The same 68 pair solves with the persistent iteration loop (svs_tvl1_plan_set_persistent:
+    every iteration of a warp at a level in one cooperative launch), on the level variants of the
+    headline run: pairs/s over 2 timed solves, the graph's kernel nodes, and whether the flows are
+    bitwise those of the headline run (ref_host, pinned host copies of its flows)."""
+    import torch
+    solver = _solver(dev, storage)
+    n = len(pairs)
+    plan = solver.plan_for([SHAPE] * n)
+    for level, tid in enumerate(level_tiles):
+        plan.set_level_tile(level, tid)
+    plan.set_persistent(True)
+    outs = torch.empty((n,) + SHAPE + (3,), dtype=torch.float32, device=dev)
+    I0s, I1s = [d_seq[a] for a, b in pairs], [d_seq[b] for a, b in pairs]
+    ms, clocks = _timed_solves(plan, I0s, I1s, [outs[i] for i in range(n)], 2, 1, dev)
+    plan.check()
+    out = {"value": n / (ms / 1000.0), "unit": "pairs/s", "ms_per_step": ms, "steps": 2,
+           "what": "the 68 pair solves alone (no mask propagation), persistent iteration loop",
+           "graph_kernels_per_solve": plan.graph_kernels(), "levels_persistent": plan.level_persistent(3),
+           "level_tiles": plan.level_tiles()[:3],
+           "bitwise_equal_to_headline_flows": bool(torch.equal(outs.cpu(), ref_host)), "clocks": clocks}
+    plan.close()
+    solver._plans.clear()
+    return out
+
+
 # ----------------------------------------------------------------- further workloads (1 GPU)
 def _solver(dev, storage):
     from singleventriclesegmentation_b200.tvl13d import TVL13DOpticalFlow
@@ -477,7 +506,7 @@ def run_mixed(args):
         solver = _solver(dev, storage)
         plan = solver.plan_for(dims)
         if not args.no_autotune:
-            tune_plan(plan, storage)
+            tune_plan(plan, storage, per_class=True)   # the 80^3 and the 128^3 pairs are two size classes
         ms, clocks = _timed_solves(plan, I0s, I1s, outs, args.steps, args.warmup, dev)
         epe, dices = {}, {}
         for i in subset:
@@ -493,6 +522,8 @@ def run_mixed(args):
         out.append({"storage": storage, "pairs_per_s": len(dims) / (ms / 1000.0), "ms_per_step": ms,
                     "equivalent_80cube_pairs_per_s": vox / 512000.0 / (ms / 1000.0), "epe_vs_fp64_oracle": epe,
                     "warped_mask_dice_vs_fp64_oracle": dices, "level_tiles": plan.level_tiles()[:3],
+                    "class_tiles": {str(l): {str(w): t for w, t in c.items()}
+                                    for l, c in getattr(plan, "class_tiles", {}).items()},
                     "clocks": clocks})
         plan.close()
         solver._plans.clear()
@@ -747,6 +778,10 @@ def main():
     if rank == 0 and world == 1 and not args.no_fp32:
         fp32 = fp32_storage_rate(dev, d_seq, pairs, args)
 
+    persistent = None
+    if rank == 0 and world == 1 and not args.no_persistent:
+        persistent = persistent_form_rate(dev, d_seq, pairs, args.storage, plan.level_tiles()[:3], host_flows)
+
     plain = None
     if rank == 0 and world == 1 and not args.no_plain_form:
         plain = plain_form_rate(dev, d_seq)
@@ -776,7 +811,7 @@ def main():
                                    % plan.level_tiles()[0],
                          "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": it_ms},
             "cpu_baseline": cpu, "plain_gpu_form": plain, "clocks": clock_info, "latency": latency,
-            "fp32_storage": fp32, "compute_metrics": mask_metrics,
+            "fp32_storage": fp32, "persistent_form": persistent, "compute_metrics": mask_metrics,
             "graph_kernels_per_solve": plan.graph_kernels,
         }
         print(json.dumps(line), flush=True)

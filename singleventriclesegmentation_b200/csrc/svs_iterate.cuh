@@ -116,12 +116,16 @@ __device__ __forceinline__ void dual_row(const T D[6], T ex, T ey, T ez, T& p0, 
 
 // Step length along g of the L1 shrinkage, the three cases of opticalFlowOps.cu:140-171 (no
 // divergence): rho < -th: +factor; rho > th: -factor; |rho| <= th: -rho/|g|^2 (0 where
-// |g|^2 <= 1e-10, the reference's (double)g2 > 1e-10 for a float g2). The division is IEEE
-// round-to-nearest like the reference's; the reference divides each component's product,
-// (-rho g_c)/|g|^2, where this step divides once and the caller multiplies by g_c.
+// |g|^2 <= 1e-10, the reference's (double)g2 > 1e-10 for a float g2). The reference divides
+// each component's product, (-rho g_c)/|g|^2, with IEEE division; this step divides once, with
+// the fast approximate divide (__fdividef, within 2 ulp for these operands), only in the lanes
+// whose |rho| is within the threshold, and the caller multiplies by g_c. Measured on the 68-pair
+// 80^3 level-0 launch: 4.4% faster than an IEEE divide (__fdiv_rn) computed for every lane.
 __device__ __forceinline__ float shrink_step(float rho, float g2s, float factor) {
   const float th = __fmul_rn(factor, g2s);
-  return (rho < -th) ? factor : (rho > th) ? -factor : (g2s >= 1e-10f ? __fdiv_rn(-rho, g2s) : 0.f);
+  float t = (rho < -th) ? factor : (rho > th) ? -factor : 0.f;
+  if (!(rho < -th) && !(rho > th) && g2s >= 1e-10f) t = __fdividef(-rho, g2s);
+  return t;
 }
 __device__ __forceinline__ float2 shrink_step(float2 rho, float2 g2s, float factor) {
   return make_float2(shrink_step(rho.x, g2s.x, factor), shrink_step(rho.y, g2s.y, factor));
