@@ -392,7 +392,7 @@ def persistent_form_rate(dev, d_seq, pairs, storage, level_tiles, ref_host):
     plan.check()
     out = {"value": n / (ms / 1000.0), "unit": "pairs/s", "ms_per_step": ms, "steps": 2,
            "what": "the 68 pair solves alone (no mask propagation), persistent iteration loop",
-           "graph_kernels_per_solve": plan.graph_kernels(), "levels_persistent": plan.level_persistent(3),
+           "graph_kernels_per_solve": plan.graph_kernels, "levels_persistent": plan.level_persistent(3),
            "level_tiles": plan.level_tiles()[:3],
            "bitwise_equal_to_headline_flows": bool(torch.equal(outs.cpu(), ref_host)), "clocks": clocks}
     plan.close()
