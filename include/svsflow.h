@@ -254,6 +254,12 @@ svs_status svs_tvl1_plan_get_residuals(svs_plan* plan, float* out_host, size_t c
  * SVS_ERR_INVALID_ARG for an unknown id. No counterpart in the reference (a query for the
  * autotuner and tests). */
 svs_status svs_tvl1_tile_info(int tile_id, int* tx, int* ty, int* dist, int* form, int* lane_voxels);
+/* CTAs of split-role variant tile_id that one SM holds at once for a storage mode (the occupancy
+ * calculator on the current device, with the kernel's registers and shared memory); general
+ * boundary != 0 for the NEAREST / periodic kernels, 0 for MIRROR. SVS_ERR_UNSUPPORTED for a
+ * variant not compiled for the storage or not fitting shared memory. No counterpart in the
+ * reference (a query for tests and tuning). */
+svs_status svs_tvl1_tile_occupancy(int storage, int tile_id, int general_boundary, int* ctas_per_sm);
 
 /* A plan sized by capacity for svs_tvl1_plan_retarget (no counterpart in the reference): room for
  * up to max_pairs pairs and at least arena_bytes of device state (the per-pair state of a level-0

@@ -90,6 +90,7 @@ _SIGS = {
     "svs_tvl1_plan_get_residuals": (c_int, [c_void_p, c_void_p, c_size_t]),
     "svs_tvl1_tile_info": (c_int, [c_int, ctypes.POINTER(c_int), ctypes.POINTER(c_int), ctypes.POINTER(c_int),
                                    ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
+    "svs_tvl1_tile_occupancy": (c_int, [c_int, c_int, c_int, ctypes.POINTER(c_int)]),
     "svs_tvl1_solve_batch": (c_int, [c_void_p, ctypes.POINTER(PairDesc), c_int, c_void_p]),
     "svs_tvl1_bench_iterations": (c_int, [c_void_p, c_int, c_int, c_void_p]),
     "svs_tvl1_plan_graph_kernels": (ctypes.c_uint64, [c_void_p]),
@@ -166,6 +167,13 @@ def tile_info(tile_id: int) -> dict:
     check(lib().svs_tvl1_tile_info(int(tile_id), *[ctypes.byref(x) for x in v]))
     return {"tx": v[0].value, "ty": v[1].value, "dist": v[2].value,
             "form": ("plain", "tma", "split")[v[3].value], "lane_voxels": v[4].value}
+
+
+def tile_occupancy(storage: int, tile_id: int, general_boundary: bool = False) -> int:
+    """CTAs of a split-role variant one SM holds at once for a storage mode (current device)."""
+    n = c_int()
+    check(lib().svs_tvl1_tile_occupancy(int(storage), int(tile_id), int(bool(general_boundary)), ctypes.byref(n)))
+    return n.value
 
 
 def auto_tiles(storage: int, dims, sms: int):

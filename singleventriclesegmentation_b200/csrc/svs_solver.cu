@@ -1326,6 +1326,23 @@ svs_status svs_tvl1_tile_info(int tile_id, int* tx, int* ty, int* dist, int* for
   return SVS_OK;
 }
 
+svs_status svs_tvl1_tile_occupancy(int storage, int tile_id, int general_boundary, int* ctas_per_sm) {
+  SVS_REQUIRE(tile_id >= 1 && tile_id <= kNumTileShapes, "svs_tvl1_tile_occupancy: unknown tile id");
+  SVS_REQUIRE(storage >= SVS_STORAGE_F32 && storage <= SVS_STORAGE_F16_FLOW32, "svs_tvl1_tile_occupancy: unknown storage");
+  SVS_REQUIRE(ctas_per_sm, "svs_tvl1_tile_occupancy: null output");
+  const TileShape& t = kTileShapes[tile_id - 1];
+  SVS_REQUIRE(t.form == kSplit, "svs_tvl1_tile_occupancy: split-role variants only");
+  const bool gen = general_boundary != 0;
+  int box[4] = {0, 0, 0, 0};
+  // op 0 sets the kernels' shared-memory attribute, which the occupancy query (op 2) needs
+  if (!split_variant(storage, t.split, 0, gen, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, box))
+    return fail(SVS_ERR_UNSUPPORTED, "svs_tvl1_tile_occupancy: variant not compiled for this storage, or its shared memory does not fit");
+  if (!split_variant(storage, t.split, 2, gen, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, box))
+    return fail(SVS_ERR_CUDA, "svs_tvl1_tile_occupancy: occupancy query failed");
+  *ctas_per_sm = box[0];
+  return SVS_OK;
+}
+
 svs_status svs_tvl1_plan_create(const svs_tvl1_params* prm, int num_pairs, const int* dims,
                                 svs_plan** out) {
   SVS_REQUIRE(prm && dims && out, "svs_tvl1_plan_create: null pointer");

@@ -184,6 +184,30 @@ def test_pair_variant_groups_run_concurrently_with_the_same_result(cuda):
     plan.check()
 
 
+def test_pair_shapes_keep_two_ctas_per_sm(cuda):
+    """The voxel-pair variants that the automatic choice runs where the GPU is full (40x8 in row
+    pairs and 32x8) fit two CTAs per SM for every 2-byte storage mode: their register and
+    shared-memory budgets are sized for it, and a kernel change that took one over the register
+    budget would halve its occupancy without changing any result (a branch in the shrinkage step
+    once took the 32x8 pair kernel to 202 registers, one CTA per SM)."""
+    from singleventriclesegmentation_b200 import _lib
+
+    def tid(tx, ty, v):
+        for t in range(1, _lib.lib().svs_tvl1_num_tiles() + 1):
+            i = _lib.tile_info(t)
+            if i["form"] == "split" and (i["tx"], i["ty"], i["lane_voxels"]) == (tx, ty, v):
+                return t
+
+    pairs40 = _lib.auto_tiles(4, [(80, 80, 80)] * 68, 148)[0]
+    pairs32, single32, single16 = tid(32, 8, 2), tid(32, 8, 1), tid(16, 16, 1)
+    for storage in (1, 2, 3, 4):   # bf16, f16, bf16-flow32, f16-flow32
+        occ = {t: _lib.tile_occupancy(storage, t) for t in (pairs40, pairs32, single32, single16)}
+        print("storage", storage, "CTAs per SM", occ)
+        assert occ[pairs40] >= 2 and occ[pairs32] >= 2, occ
+        assert min(occ.values()) >= 1
+    assert _lib.tile_occupancy(0, tid(32, 16, 2)) >= 1   # FP32 fields: 32x16 pairs
+
+
 def test_automatic_pair_variants_keep_the_result(cuda):
     """At a level whose column tiles fill the GPU twice over, the automatic choice gives the pairs
     of each width the variant with the least modelled work (svs_tvl1_auto_tiles) and the plan runs
