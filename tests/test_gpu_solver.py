@@ -184,9 +184,9 @@ def test_pair_variant_groups_run_concurrently_with_the_same_result(cuda):
     plan.check()
 
 
-def test_pair_shapes_keep_two_ctas_per_sm(cuda):
-    """The voxel-pair variants that the automatic choice runs where the GPU is full (40x8 in row
-    pairs and 32x8) fit two CTAs per SM for every 2-byte storage mode: their register and
+def test_automatic_shapes_keep_two_ctas_per_sm(cuda):
+    """The variants of the automatic choice for 2-byte fields (40x8 and 32x8 voxel pairs, 32x8 and
+    16x16 single voxels) fit two CTAs per SM for every 2-byte storage mode: their register and
     shared-memory budgets are sized for it, and a kernel change that took one over the register
     budget would halve its occupancy without changing any result (a branch in the shrinkage step
     once took the 32x8 pair kernel to 202 registers, one CTA per SM)."""
@@ -203,8 +203,7 @@ def test_pair_shapes_keep_two_ctas_per_sm(cuda):
     for storage in (1, 2, 3, 4):   # bf16, f16, bf16-flow32, f16-flow32
         occ = {t: _lib.tile_occupancy(storage, t) for t in (pairs40, pairs32, single32, single16)}
         print("storage", storage, "CTAs per SM", occ)
-        assert occ[pairs40] >= 2 and occ[pairs32] >= 2, occ
-        assert min(occ.values()) >= 1
+        assert min(occ.values()) >= 2, occ
     assert _lib.tile_occupancy(0, tid(32, 16, 2)) >= 1   # FP32 fields: 32x16 pairs
 
 
