@@ -783,10 +783,10 @@ struct AutoCost {
   int tid;
   float ns;  // per column-tile plane
 };
-// 40x8 voxel pairs in row pairs 6.22-6.42 ns (320 voxels), 32x8 voxel pairs 5.01-5.14 ns (256
-// voxels), 16x16 single voxels 6.11-6.19 ns (256 voxels): per voxel the first two are alike
-// (~20 ps) and the third 20% slower
-constexpr AutoCost kAutoCosts16[] = {{kAuto16W40, 6.35f}, {split_id(32, 8, 3, 2), 5.10f}, {kAuto16, 6.15f}};
+// f16-flow32 and bf16-flow32: 40x8 voxel pairs in row pairs 5.96-6.32 ns (320 voxels), 32x8
+// voxel pairs 5.05-5.28 ns (256 voxels), 16x16 single voxels 5.90-6.09 ns (256 voxels): per voxel
+// the first two are alike (~19-20 ps) and the third 15% slower
+constexpr AutoCost kAutoCosts16[] = {{kAuto16W40, 6.13f}, {split_id(32, 8, 3, 2), 5.20f}, {kAuto16, 6.00f}};
 constexpr int kAutoWaves = 2;  // waves of 40x8 column tiles (two CTAs per SM) for the per-pair choice
 
 int auto_choice(int storage, int n, const int* dims, int sms, int* pair_tid) {
