@@ -276,7 +276,7 @@ def tune_plan(plan, storage: str, levels: int = 3, per_class: bool = False):
     from singleventriclesegmentation_b200 import _lib, autotune
     n = int(_lib.lib().svs_tvl1_num_tiles())
     cands = [t for t in range(1, n + 1) if _lib.tile_info(t)["form"] != "plain"]
-    return autotune.tune(plan, storage, levels, candidates=cands, use_cache=False, iters=6, per_class=per_class)
+    return autotune.tune(plan, storage, levels, candidates=cands, use_cache=False, iters=12, per_class=per_class)
 
 
 def iterate_roofline(plan, storage: str, level_voxels: int, stream, dev):
